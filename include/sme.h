@@ -1,0 +1,226 @@
+/*
+ * sme.h -- C-ABI of the B200 subgraph-enumeration engine (libsme.so).
+ *
+ * Drop-in boundary for the GPU enumeration path of guowentian/SubgraphMatchGPU.
+ * Every entry point takes plain pointers and sizes; no C++ or torch types
+ * cross this boundary.  All calls return an sme_status; the library never
+ * exits or aborts the caller (the reference calls exit(-1) from CUDA_ERROR,
+ * src/gpu/utils/GPUUtil.cuh:9-17, and asserts elsewhere).
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   graph loading      src/graph/GraphIO.h:26-136 (ReadDataFile/ReadCSRBinFile)
+ *   graph writing      src/graph/GraphIO.h:356-387 (WriteCSRBinFile)
+ *   preprocessing      src/preprocess/PreprocessGraph.h:13-95
+ *   instance wiring    src/gpu/PatternMatchGPUInstance.cuh:26-176 (InitGPUInstance)
+ *   execution          src/gpu/executor/PatternMatch.cuh:52-88 (Execute), the
+ *                      plugin HybridGPUComponent (src/gpu/impl/common/HybridGPUComp.cuh:18-107)
+ *                      and HybridGPUProcessor::ProcessLevel
+ *                      (src/gpu/impl/common/HybridGPUProcessor.cuh:14-50)
+ *   plan printing      src/query/TestPlan.cpp:8-51
+ */
+#ifndef SME_H_
+#define SME_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace assert/exit in the reference) ---------------- */
+typedef enum sme_status {
+  SME_OK = 0,
+  SME_ERR_INVALID_ARG = 1,
+  SME_ERR_BAD_FILE = 2,
+  SME_ERR_OOM = 3,
+  SME_ERR_TIMEOUT = 4,
+  SME_ERR_CUDA = 5,
+  SME_ERR_UNSUPPORTED_QUERY = 6,
+  SME_ERR_NO_DEVICE = 7,
+  SME_ERR_CAPACITY = 8,  /* enumeration output buffer too small           */
+  SME_ERR_BUSY = 9,      /* server queue full / request not finished yet  */
+  SME_ERR_CANCELLED = 10
+} sme_status;
+
+/* ---- enums: same numeric values as src/Meta.h:47-124 -------------------- */
+enum {
+  SME_CPU_WCOJ = 0, SME_CPU_VF2 = 1, SME_CPU_BFS = 2, SME_CPU_RBFS = 3,
+  SME_GPU_GPSM = 4, SME_GPU_GPSM_REUSE = 5, SME_GPU_LIGHT = 6
+};
+enum { SME_HYBRID_CPU_GPU = 0, SME_IN_MEMORY_GPU = 1, SME_EXTERNAL_GPU = 2 };
+enum { SME_EXT_CACHE = 0, SME_EXT_UMA = 1 };
+/* LazyTraversalCompressLevel, src/query/common/LazyTraversalCommon.h:38-76 */
+enum {
+  SME_COMPRESS_MATERIALIZE = 0,
+  SME_COMPRESS_NON_MATERIALIZE = 1,
+  SME_COMPRESS_NON_MATERIALIZE_OPT = 2,
+  SME_COMPRESS_SPECIAL = 3
+};
+#define SME_NUM_QUERIES 14 /* Q0..Q13 */
+
+typedef struct sme_graph sme_graph; /* opaque: host CSR + cached device copy */
+
+/* Options of one enumeration run; mirrors the patternmatchgpu flags
+ * (src/gpu/PatternMatchGPU.cu:17-37). */
+typedef struct sme_opts {
+  int32_t query_type;      /* -q : 0..13                                     */
+  int32_t algo;            /* -a : 4 GPU_GPSM, 5 GPU_GPSM_REUSE, 6 GPU_LIGHT */
+  int32_t execute_mode;    /* -m : 1 IN_MEMORY_GPU, 2 EXTERNAL_GPU           */
+  int32_t compress_level;  /* -c : 0..3, default 3 (SPECIAL)                 */
+  int32_t enable_ordering; /* -r : 1 (default) keeps symmetry breaking       */
+  int32_t ext_variant;     /* -y : 0 EXT_CACHE, 1 EXT_UMA                    */
+  int32_t reuse_autogen;   /* 0 hard-coded reuse plan, 1 cost-based autogen,
+                              -1 (default) hard-coded when one exists       */
+  int32_t device;          /* CUDA device ordinal                            */
+  uint64_t mem_limit_bytes;/* device budget for frontiers+graph; 0 = auto    */
+  uint64_t root_begin;     /* first-level vertex range [begin,end) (a task   */
+  uint64_t root_end;       /*  of IntraPartScheduler); end==0 means all      */
+  int32_t warp_granularity;/* 0 auto, 1 warp per path only (tuning knob)     */
+  int32_t reserved[7];
+} sme_opts;
+
+/* Counters of the last sme_count/sme_enumerate call on this thread. */
+typedef struct sme_stats {
+  double elapsed_ms;          /* plan + device execution (+ graph H2D when it
+                                 was not resident), as elapsed_time= in the
+                                 reference (PatternMatch.cuh:77-87)          */
+  double kernel_ms;           /* sum of CUDA-event time of the hot kernels   */
+  uint64_t kernel_launches;   /* kernels of this library launched            */
+  uint64_t batches;           /* level batches processed                    */
+  uint64_t algorithmic_bytes; /* merge-bound bytes of all intersection steps */
+  uint64_t h2d_bytes;         /* host->device bytes moved by this call       */
+  uint64_t d2h_bytes;
+  uint64_t peak_device_bytes; /* high-water mark of the frontier arena       */
+  uint64_t paths_processed;   /* partial instances entering compute steps    */
+} sme_stats;
+
+/* ---- options ------------------------------------------------------------- */
+sme_status sme_opts_default(sme_opts* opts);
+
+/* ---- graphs (GraphIO.h / PreprocessGraph.h) ------------------------------ */
+/* BIN CSR: 4 x size_t header (4, 8, n, m), uint64 row_ptrs[n+1], uint32 cols[m]
+ * (GraphIO.h:88-136).  Read with one bulk read, validated. */
+sme_status sme_graph_load_bin(const char* path, sme_graph** out);
+/* SNAP edge list text (GraphIO.h:195-270); directed=0 stores both directions;
+ * adjacency lists are sorted.  No preprocessing. */
+sme_status sme_graph_load_snap(const char* path, int directed, sme_graph** out);
+/* Dispatch on the file suffix like GraphIO::ReadDataFile (GraphIO.h:48-64). */
+sme_status sme_graph_load(const char* path, int directed, sme_graph** out);
+/* From caller CSR.  copy=1 copies; copy=0 borrows (caller keeps the arrays
+ * alive and unchanged until sme_graph_free). */
+sme_status sme_graph_from_csr(const uint64_t* row_ptrs, const uint32_t* cols,
+                              uint64_t n, uint64_t m, int copy,
+                              sme_graph** out);
+sme_status sme_graph_info(const sme_graph* g, uint64_t* n, uint64_t* m,
+                          uint64_t* max_degree);
+sme_status sme_graph_csr(const sme_graph* g, const uint64_t** row_ptrs,
+                         const uint32_t** cols);
+/* Writes exactly the bytes of GraphIO::WriteCSRBinFile to `path`. */
+sme_status sme_graph_write_bin(const sme_graph* g, const char* path);
+/* PreprocessGraph::Preprocess: drop self loops and parallel edges, then
+ * dangling vertices with a dense order-preserving relabel. */
+sme_status sme_graph_preprocess(sme_graph* g);
+/* GraphIO::Validate: sorted, no self loop, no parallel edge, no dangling. */
+sme_status sme_graph_validate(const sme_graph* g);
+/* Copies the CSR to device memory of `device` and keeps it there; later runs
+ * on that device reuse it (inputs resident in HBM). */
+sme_status sme_graph_to_device(sme_graph* g, int device);
+sme_status sme_graph_release_device(sme_graph* g);
+sme_status sme_graph_free(sme_graph* g);
+
+/* ---- seeded synthetic graphs (all passed through the preprocess step) ---- */
+/* R-MAT(scale, edge_factor, a, b, c) with d = 1-a-b-c; undirected. */
+sme_status sme_generate_rmat(int32_t scale, int32_t edge_factor, double a,
+                             double b, double c, uint64_t seed,
+                             sme_graph** out);
+/* Erdos-Renyi G(n, p = avg_degree/(n-1)). */
+sme_status sme_generate_er(uint64_t n, double avg_degree, uint64_t seed,
+                           sme_graph** out);
+/* Barabasi-Albert with m_attach edges per new vertex. */
+sme_status sme_generate_ba(uint64_t n, uint32_t m_attach, uint64_t seed,
+                           sme_graph** out);
+/* Complete graph K_n (GenerateNClique, src/test/gpu/TestGPUCommon.cuh:32-49). */
+sme_status sme_generate_clique(uint64_t n, sme_graph** out);
+
+/* ---- enumeration (PatternMatch::Execute) --------------------------------- */
+sme_status sme_count(sme_graph* g, const sme_opts* opts, uint64_t* count);
+/* Writes up to cap instances, each query_vertex_count uint32 ids in pattern
+ * vertex order (u0..u_{k-1}); *n_out = number of instances found (the call
+ * fails with SME_ERR_CAPACITY when it exceeds cap, *n_out still valid). */
+sme_status sme_enumerate(sme_graph* g, const sme_opts* opts, uint32_t* out,
+                         uint64_t cap_instances, uint64_t* n_out);
+/* Stats of the last sme_count/sme_enumerate issued by this thread. */
+sme_status sme_last_stats(sme_stats* stats);
+/* Number of pattern vertices of query q (Query.h:84-434). */
+int32_t sme_query_vertex_count(int32_t query_type);
+
+/* ---- plans (TestPlan.cpp) ------------------------------------------------ */
+/* plan_type: 0 TraversalPlan, 1 ReuseTraversalPlan (autogen as test_plan -t 1),
+ * 2 LazyTraversalPlan (NON_MATERIALIZE_OPT as test_plan -t 2),
+ * 3 ReuseTraversalPlan with the hard-coded plan (patternmatch default),
+ * 4 LazyTraversalPlan with compress_level SPECIAL.
+ * Writes a NUL-terminated text description; returns SME_ERR_CAPACITY when
+ * `cap` is too small (*needed holds the size). */
+sme_status sme_plan_describe(int32_t query_type, int32_t plan_type, char* buf,
+                             uint64_t cap, uint64_t* needed);
+
+/* ---- batched form: many small graphs, one persistent launch ------------- */
+typedef struct sme_batch_opts {
+  int32_t device;
+  int32_t autotune;        /* 1: pick granularity/block shape by measuring   */
+  int32_t granularity;     /* 0 auto, 1 warp per root, 2 CTA per root        */
+  int32_t block_threads;   /* 0 auto                                         */
+  int32_t use_graph;       /* 1: capture the launch in a CUDA graph          */
+  int32_t reserved[11];
+} sme_batch_opts;
+sme_status sme_batch_opts_default(sme_batch_opts* o);
+/* counts[i] = count of queries[i] on graphs[i] (symmetry-broken, uint64). */
+sme_status sme_batch_count(sme_graph* const* graphs, const int32_t* queries,
+                           uint64_t num, const sme_batch_opts* opts,
+                           uint64_t* counts);
+typedef struct sme_batch_plan sme_batch_plan; /* resident packed batch */
+sme_status sme_batch_prepare(sme_graph* const* graphs, const int32_t* queries,
+                             uint64_t num, const sme_batch_opts* opts,
+                             sme_batch_plan** out);
+sme_status sme_batch_run(sme_batch_plan* p, uint64_t* counts, double* ms);
+sme_status sme_batch_describe(const sme_batch_plan* p, int32_t* granularity,
+                              int32_t* block_threads, uint64_t* work_items);
+sme_status sme_batch_free(sme_batch_plan* p);
+
+/* ---- served form: resident graphs + continuous batching ----------------- */
+typedef struct sme_server sme_server;
+typedef struct sme_server_opts {
+  int32_t device;
+  int32_t slots;             /* concurrent requests on the device           */
+  uint64_t mem_budget_bytes; /* admission budget (estimated frontier bytes) */
+  int32_t queue_capacity;
+  int32_t reserved[9];
+} sme_server_opts;
+sme_status sme_server_opts_default(sme_server_opts* o);
+sme_status sme_server_create(const sme_server_opts* o, sme_server** out);
+/* Keeps `g` resident on the server's device; returns its graph id. */
+sme_status sme_server_add_graph(sme_server* s, sme_graph* g, int32_t* gid);
+/* Enqueue a request on a resident graph (gid) or on an attached graph
+ * (gid = -1, `attached` non-NULL, owned by the caller until completion). */
+sme_status sme_server_submit(sme_server* s, int32_t gid, sme_graph* attached,
+                             const sme_opts* opts, uint64_t* request_id);
+/* Non-blocking: SME_ERR_BUSY while pending; else the request's final status,
+ * its count and its latency (submit -> result) in milliseconds. */
+sme_status sme_server_poll(sme_server* s, uint64_t request_id, uint64_t* count,
+                           double* latency_ms);
+sme_status sme_server_wait(sme_server* s, uint64_t request_id,
+                           uint64_t* count, double* latency_ms);
+sme_status sme_server_stats(sme_server* s, uint64_t* completed,
+                            uint64_t* max_inflight, uint64_t* rejected);
+sme_status sme_server_destroy(sme_server* s);
+
+/* ---- errors --------------------------------------------------------------- */
+/* Message of the last failing call on this thread ("" if none). */
+const char* sme_last_error(void);
+const char* sme_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SME_H_ */

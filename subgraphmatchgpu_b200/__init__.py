@@ -1,0 +1,295 @@
+"""Python binding of libsme, the B200 subgraph-enumeration engine.
+
+The engine is a drop-in for the GPU enumeration path of
+guowentian/SubgraphMatchGPU: the query registry Q0..Q13 with the reference's
+symmetry-breaking order (src/query/common/Query.h), the plain-BFS, LIGHT and
+reuse-BFS plans (src/query/*Plan.h), the BIN CSR format
+(src/graph/GraphIO.h:88-136) and the ``patternmatchgpu`` flags
+(src/gpu/PatternMatchGPU.cu:17-37).  This module is a thin ctypes layer over
+the C-ABI declared in include/sme.h; every call goes to the compiled library
+and raises SmeError on a non-zero status.  There is no Python or CPU fallback:
+without libsme.so (or without a GPU for the device entry points) calls fail.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsme.so")
+
+# algorithms / modes (src/Meta.h:47-77)
+GPU_GPSM, GPU_GPSM_REUSE, GPU_LIGHT = 4, 5, 6
+IN_MEMORY_GPU, EXTERNAL_GPU = 1, 2
+EXT_CACHE, EXT_UMA = 0, 1
+COMPRESS_MATERIALIZE, COMPRESS_NON_MATERIALIZE, COMPRESS_NON_MATERIALIZE_OPT, COMPRESS_SPECIAL = 0, 1, 2, 3
+QUERY_NAMES = {
+    0: "triangle", 1: "4-cycle", 2: "diamond", 3: "4-clique", 4: "house", 5: "quad-triangle",
+    6: "near-5-clique", 7: "5-clique", 8: "chordal-roof", 9: "three-triangle", 10: "solar-square",
+    11: "6-clique", 12: "near-near-5-clique", 13: "triangle-in-diamond",
+}
+
+STATUS = {
+    0: "OK", 1: "INVALID_ARG", 2: "BAD_FILE", 3: "OOM", 4: "TIMEOUT", 5: "CUDA", 6: "UNSUPPORTED_QUERY",
+    7: "NO_DEVICE", 8: "CAPACITY", 9: "BUSY", 10: "CANCELLED",
+}
+
+
+class SmeError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("query_type", C.c_int32), ("algo", C.c_int32), ("execute_mode", C.c_int32),
+        ("compress_level", C.c_int32), ("enable_ordering", C.c_int32), ("ext_variant", C.c_int32),
+        ("reuse_autogen", C.c_int32), ("device", C.c_int32), ("mem_limit_bytes", C.c_uint64),
+        ("root_begin", C.c_uint64), ("root_end", C.c_uint64), ("warp_granularity", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("elapsed_ms", C.c_double), ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64),
+        ("batches", C.c_uint64), ("algorithmic_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64),
+        ("d2h_bytes", C.c_uint64), ("peak_device_bytes", C.c_uint64), ("paths_processed", C.c_uint64),
+    ]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32), ("autotune", C.c_int32), ("granularity", C.c_int32),
+        ("block_threads", C.c_int32), ("use_graph", C.c_int32), ("reserved", C.c_int32 * 11),
+    ]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32), ("slots", C.c_int32), ("mem_budget_bytes", C.c_uint64),
+        ("queue_capacity", C.c_int32), ("reserved", C.c_int32 * 9),
+    ]
+
+
+# Every entry point of include/sme.h with its ctypes signature.
+_P = C.c_void_p
+_PP = C.POINTER(C.c_void_p)
+_U64 = C.c_uint64
+_PU64 = C.POINTER(C.c_uint64)
+SIGNATURES = {
+    "sme_opts_default": (C.c_int, [C.POINTER(Opts)]),
+    "sme_graph_load_bin": (C.c_int, [C.c_char_p, _PP]),
+    "sme_graph_load_snap": (C.c_int, [C.c_char_p, C.c_int, _PP]),
+    "sme_graph_load": (C.c_int, [C.c_char_p, C.c_int, _PP]),
+    "sme_graph_from_csr": (C.c_int, [_P, _P, _U64, _U64, C.c_int, _PP]),
+    "sme_graph_info": (C.c_int, [_P, _PU64, _PU64, _PU64]),
+    "sme_graph_csr": (C.c_int, [_P, _PP, _PP]),
+    "sme_graph_write_bin": (C.c_int, [_P, C.c_char_p]),
+    "sme_graph_preprocess": (C.c_int, [_P]),
+    "sme_graph_validate": (C.c_int, [_P]),
+    "sme_graph_to_device": (C.c_int, [_P, C.c_int]),
+    "sme_graph_release_device": (C.c_int, [_P]),
+    "sme_graph_free": (C.c_int, [_P]),
+    "sme_generate_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, _U64, _PP]),
+    "sme_generate_er": (C.c_int, [_U64, C.c_double, _U64, _PP]),
+    "sme_generate_ba": (C.c_int, [_U64, C.c_uint32, _U64, _PP]),
+    "sme_generate_clique": (C.c_int, [_U64, _PP]),
+    "sme_count": (C.c_int, [_P, C.POINTER(Opts), _PU64]),
+    "sme_enumerate": (C.c_int, [_P, C.POINTER(Opts), _P, _U64, _PU64]),
+    "sme_last_stats": (C.c_int, [C.POINTER(Stats)]),
+    "sme_query_vertex_count": (C.c_int32, [C.c_int32]),
+    "sme_plan_describe": (C.c_int, [C.c_int32, C.c_int32, C.c_char_p, _U64, _PU64]),
+    "sme_batch_opts_default": (C.c_int, [C.POINTER(BatchOpts)]),
+    "sme_batch_count": (C.c_int, [_P, _P, _U64, C.POINTER(BatchOpts), _P]),
+    "sme_batch_prepare": (C.c_int, [_P, _P, _U64, C.POINTER(BatchOpts), _PP]),
+    "sme_batch_run": (C.c_int, [_P, _P, C.POINTER(C.c_double)]),
+    "sme_batch_describe": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _PU64]),
+    "sme_batch_free": (C.c_int, [_P]),
+    "sme_server_opts_default": (C.c_int, [C.POINTER(ServerOpts)]),
+    "sme_server_create": (C.c_int, [C.POINTER(ServerOpts), _PP]),
+    "sme_server_add_graph": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
+    "sme_server_submit": (C.c_int, [_P, C.c_int32, _P, C.POINTER(Opts), _PU64]),
+    "sme_server_poll": (C.c_int, [_P, _U64, _PU64, C.POINTER(C.c_double)]),
+    "sme_server_wait": (C.c_int, [_P, _U64, _PU64, C.POINTER(C.c_double)]),
+    "sme_server_stats": (C.c_int, [_P, _PU64, _PU64, _PU64]),
+    "sme_server_destroy": (C.c_int, [_P]),
+    "sme_last_error": (C.c_char_p, []),
+    "sme_version": (C.c_char_p, []),
+}
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Loads libsme.so (built in-tree); raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `make -C subgraphmatchgpu_b200/csrc` first")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(st: int) -> None:
+    if st != 0:
+        raise SmeError(st, lib().sme_last_error().decode())
+
+
+def opts(query: int = 0, algo: int = GPU_LIGHT, mode: int = IN_MEMORY_GPU, **kw) -> Opts:
+    o = Opts()
+    _check(lib().sme_opts_default(C.byref(o)))
+    o.query_type, o.algo, o.execute_mode = query, algo, mode
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def query_vertex_count(q: int) -> int:
+    return lib().sme_query_vertex_count(q)
+
+
+def plan_describe(q: int, plan_type: int) -> str:
+    need = C.c_uint64(0)
+    lib().sme_plan_describe(q, plan_type, None, 0, C.byref(need))
+    buf = C.create_string_buffer(need.value)
+    _check(lib().sme_plan_describe(q, plan_type, buf, need.value, C.byref(need)))
+    return buf.value.decode()
+
+
+def last_stats() -> Stats:
+    s = Stats()
+    _check(lib().sme_last_stats(C.byref(s)))
+    return s
+
+
+class Graph:
+    """Owned handle of a host CSR graph (optionally resident on a device)."""
+
+    def __init__(self, handle: int, keep=None):
+        self._h = C.c_void_p(handle)
+        self._keep = keep  # arrays borrowed by the library (copy=0)
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @classmethod
+    def load(cls, path: str, directed: int = 0) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().sme_graph_load(path.encode(), directed, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_csr(cls, row_ptrs, cols, copy: bool = True) -> "Graph":
+        rp = np.ascontiguousarray(row_ptrs, dtype=np.uint64)
+        cl = np.ascontiguousarray(cols, dtype=np.uint32)
+        h = C.c_void_p()
+        _check(lib().sme_graph_from_csr(rp.ctypes.data, cl.ctypes.data, len(rp) - 1, len(cl), int(copy),
+                                        C.byref(h)))
+        return cls(h.value, None if copy else (rp, cl))
+
+    @classmethod
+    def rmat(cls, scale: int, edge_factor: int, a=0.57, b=0.19, c=0.19, seed: int = 1) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().sme_generate_rmat(scale, edge_factor, a, b, c, seed, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def er(cls, n: int, avg_degree: float, seed: int = 1) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().sme_generate_er(n, avg_degree, seed, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def ba(cls, n: int, m_attach: int, seed: int = 1) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().sme_generate_ba(n, m_attach, seed, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def clique(cls, n: int) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().sme_generate_clique(n, C.byref(h)))
+        return cls(h.value)
+
+    def info(self):
+        n, m, d = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(lib().sme_graph_info(self._h, C.byref(n), C.byref(m), C.byref(d)))
+        return n.value, m.value, d.value
+
+    @property
+    def n(self) -> int:
+        return self.info()[0]
+
+    @property
+    def m(self) -> int:
+        return self.info()[1]
+
+    def csr(self):
+        """Copies of (row_ptrs uint64[n+1], cols uint32[m])."""
+        n, m, _ = self.info()
+        rp, cl = C.c_void_p(), C.c_void_p()
+        _check(lib().sme_graph_csr(self._h, C.byref(rp), C.byref(cl)))
+        r = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_uint64)), shape=(n + 1,)).copy()
+        c = (np.ctypeslib.as_array(C.cast(cl, C.POINTER(C.c_uint32)), shape=(m,)).copy()
+             if m else np.zeros(0, np.uint32))
+        return r, c
+
+    def write_bin(self, path: str) -> None:
+        _check(lib().sme_graph_write_bin(self._h, path.encode()))
+
+    def preprocess(self) -> None:
+        _check(lib().sme_graph_preprocess(self._h))
+
+    def validate(self) -> None:
+        _check(lib().sme_graph_validate(self._h))
+
+    def to_device(self, device: int = 0) -> None:
+        _check(lib().sme_graph_to_device(self._h, device))
+
+    def release_device(self) -> None:
+        _check(lib().sme_graph_release_device(self._h))
+
+    def count(self, query: int, algo: int = GPU_LIGHT, mode: int = IN_MEMORY_GPU, **kw) -> int:
+        o = opts(query, algo, mode, **kw)
+        out = C.c_uint64(0)
+        _check(lib().sme_count(self._h, C.byref(o), C.byref(out)))
+        return out.value
+
+    def enumerate(self, query: int, algo: int = GPU_LIGHT, cap: Optional[int] = None, **kw) -> np.ndarray:
+        """All instances as a (count, k) uint32 array (pattern-vertex order)."""
+        o = opts(query, algo, IN_MEMORY_GPU, **kw)
+        k = query_vertex_count(query)
+        if cap is None:
+            cap = self.count(query, algo, **kw)
+        buf = np.zeros((max(cap, 1), k), dtype=np.uint32)
+        got = C.c_uint64(0)
+        _check(lib().sme_enumerate(self._h, C.byref(o), buf.ctypes.data, cap, C.byref(got)))
+        return buf[: got.value]
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            lib().sme_graph_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = [
+    "Graph", "SmeError", "Opts", "Stats", "lib", "opts", "plan_describe", "last_stats", "query_vertex_count",
+    "GPU_GPSM", "GPU_GPSM_REUSE", "GPU_LIGHT", "IN_MEMORY_GPU", "EXTERNAL_GPU", "SIGNATURES", "QUERY_NAMES",
+]

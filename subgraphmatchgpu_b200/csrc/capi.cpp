@@ -1,0 +1,378 @@
+// C-ABI of libsme (include/sme.h): handles, status codes, per-thread errors.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+
+#include "engine.h"
+#include "sme_internal.h"
+
+struct sme_graph {
+  sme::HostGraph g;
+};
+
+namespace sme {
+
+static thread_local std::string t_last_error;
+static thread_local sme_stats t_last_stats{};
+
+void SetLastError(const std::string& msg) { t_last_error = msg; }
+
+template <typename F>
+static sme_status Guard(F&& f) {
+  try {
+    f();
+    t_last_error.clear();
+    return SME_OK;
+  } catch (const Error& e) {
+    t_last_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    t_last_error = "host allocation failed";
+    return SME_ERR_OOM;
+  } catch (const std::exception& e) {
+    t_last_error = e.what();
+    return SME_ERR_INVALID_ARG;
+  }
+}
+
+// One execution context per device for the synchronous API; calls on the
+// same device are serialised by its mutex.
+struct CtxSlot {
+  std::mutex mu;
+  DeviceContext* ctx = nullptr;
+  uint64_t bytes = 0;
+};
+static std::mutex g_ctx_mu;
+static std::map<int, std::unique_ptr<CtxSlot>> g_ctx;
+
+static CtxSlot& SlotFor(int device) {
+  std::lock_guard<std::mutex> l(g_ctx_mu);
+  auto& s = g_ctx[device];
+  if (!s) s.reset(new CtxSlot());
+  return *s;
+}
+
+static void CheckOpts(const sme_opts& o) {
+  if (o.query_type < 0 || o.query_type >= SME_NUM_QUERIES)
+    Fail(SME_ERR_UNSUPPORTED_QUERY, "query_type must be 0..13");
+  if (o.execute_mode == SME_HYBRID_CPU_GPU)
+    Fail(SME_ERR_INVALID_ARG, "execute_mode 0 (HYBRID_CPU_GPU) is not part of this engine; use 1 or 2");
+  if (o.execute_mode != SME_IN_MEMORY_GPU && o.execute_mode != SME_EXTERNAL_GPU)
+    Fail(SME_ERR_INVALID_ARG, "execute_mode must be 1 (IN_MEMORY_GPU) or 2 (EXTERNAL_GPU)");
+  if (o.execute_mode == SME_EXTERNAL_GPU && o.algo != SME_GPU_LIGHT)
+    Fail(SME_ERR_INVALID_ARG, "EXTERNAL_GPU runs the LIGHT plan only (algo 6)");
+}
+
+struct RunOut {
+  uint64_t count = 0;
+  uint64_t emitted = 0;
+};
+
+// Shared by sme_count / sme_enumerate.
+static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t* host_out, uint64_t cap) {
+  CheckOpts(o);
+  auto t0 = std::chrono::steady_clock::now();
+  Program prog = Compile(o, enumerate);
+  CtxSlot& slot = SlotFor(o.device);
+  std::lock_guard<std::mutex> lock(slot.mu);
+  if (!slot.ctx || (o.mem_limit_bytes && slot.bytes != o.mem_limit_bytes)) {
+    if (slot.ctx) DestroyContext(slot.ctx);
+    slot.ctx = nullptr;
+    slot.ctx = CreateContext(o.device, o.mem_limit_bytes);
+    slot.bytes = o.mem_limit_bytes;
+  }
+  DeviceContext& ctx = *slot.ctx;
+  uint64_t rb = o.root_begin, re = o.root_end ? o.root_end : g->g.n;
+  if (re > g->g.n) re = g->g.n;
+  RunResult r;
+  uint64_t h2d = 0, d2h = 8;
+  if (o.execute_mode == SME_EXTERNAL_GPU) {
+    if (enumerate) Fail(SME_ERR_INVALID_ARG, "enumeration runs in IN_MEMORY_GPU mode");
+    r = RunProgramExternal(prog, g->g, ctx, rb, re, o.ext_variant, 0);
+    h2d = r.stats.h2d_bytes;
+  } else {
+    DeviceGraph* dg = g->g.dev;
+    bool temp = false;
+    if (!dg || dg->device != o.device) {
+      dg = UploadGraph(g->g, o.device, ctx.stream, &h2d);
+      temp = true;
+    }
+    uint32_t* d_out = nullptr;
+    try {
+      if (enumerate && cap) {
+        size_t bytes = (size_t)cap * prog.n * sizeof(uint32_t);
+        if (cudaMalloc((void**)&d_out, bytes) != cudaSuccess) {
+          cudaGetLastError();
+          Fail(SME_ERR_OOM, "cannot allocate enumeration buffer");
+        }
+      }
+      r = RunProgram(prog, *dg, ctx, rb, re, d_out, cap, o.warp_granularity);
+      if (enumerate && cap && host_out) {
+        uint64_t ncopy = std::min<uint64_t>(r.emitted, cap);
+        if (ncopy) {
+          if (cudaMemcpy(host_out, d_out, ncopy * prog.n * sizeof(uint32_t), cudaMemcpyDeviceToHost) !=
+              cudaSuccess)
+            Fail(SME_ERR_CUDA, "copy of enumerated instances failed");
+          d2h += ncopy * prog.n * sizeof(uint32_t);
+        }
+      }
+    } catch (...) {
+      if (d_out) cudaFree(d_out);
+      if (temp) FreeDeviceGraph(dg);
+      throw;
+    }
+    if (d_out) cudaFree(d_out);
+    if (temp) FreeDeviceGraph(dg);
+  }
+  r.stats.h2d_bytes = h2d;
+  r.stats.d2h_bytes = d2h;
+  r.stats.elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  t_last_stats = r.stats;
+  RunOut ro;
+  ro.count = r.count;
+  ro.emitted = r.emitted;
+  return ro;
+}
+
+}  // namespace sme
+
+using namespace sme;
+
+extern "C" {
+
+sme_status sme_opts_default(sme_opts* o) {
+  if (!o) return SME_ERR_INVALID_ARG;
+  std::memset(o, 0, sizeof(*o));
+  o->query_type = 0;
+  o->algo = SME_GPU_LIGHT;
+  o->execute_mode = SME_IN_MEMORY_GPU;
+  o->compress_level = SME_COMPRESS_SPECIAL;
+  o->enable_ordering = 1;
+  o->ext_variant = SME_EXT_CACHE;
+  o->reuse_autogen = -1;
+  o->device = 0;
+  return SME_OK;
+}
+
+sme_status sme_graph_load_bin(const char* path, sme_graph** out) {
+  if (!path || !out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    std::unique_ptr<sme_graph> g(new sme_graph());
+    ReadBinFile(path, g->g);
+    *out = g.release();
+  });
+}
+
+sme_status sme_graph_load_snap(const char* path, int directed, sme_graph** out) {
+  if (!path || !out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    std::unique_ptr<sme_graph> g(new sme_graph());
+    ReadSnapFile(path, directed != 0, g->g);
+    *out = g.release();
+  });
+}
+
+sme_status sme_graph_load(const char* path, int directed, sme_graph** out) {
+  if (!path || !out) return SME_ERR_INVALID_ARG;
+  std::string p(path);
+  std::string suf = p.substr(p.rfind('.') + 1);
+  if (suf == "bin") return sme_graph_load_bin(path, out);
+  if (suf == "txt") return sme_graph_load_snap(path, directed, out);
+  SetLastError("unknown graph file suffix ." + suf + " (expected .bin or .txt)");
+  return SME_ERR_BAD_FILE;
+}
+
+sme_status sme_graph_from_csr(const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n, uint64_t m, int copy,
+                              sme_graph** out) {
+  if (!row_ptrs || (!cols && m) || !out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    if (row_ptrs[0] != 0 || row_ptrs[n] != m) Fail(SME_ERR_INVALID_ARG, "row_ptrs must span [0, m]");
+    for (uint64_t u = 0; u < n; ++u)
+      if (row_ptrs[u] > row_ptrs[u + 1]) Fail(SME_ERR_INVALID_ARG, "row_ptrs not monotone");
+    for (uint64_t j = 0; j < m; ++j)
+      if (cols[j] >= n) Fail(SME_ERR_INVALID_ARG, "column id out of range");
+    std::unique_ptr<sme_graph> g(new sme_graph());
+    if (copy) {
+      g->g.Adopt(std::vector<uintE>(row_ptrs, row_ptrs + n + 1), std::vector<uintV>(cols, cols + m));
+    } else {
+      g->g.n = n;
+      g->g.m = m;
+      g->g.row_ptrs = const_cast<uintE*>(row_ptrs);
+      g->g.cols = const_cast<uintV*>(cols);
+      g->g.borrowed = true;
+    }
+    *out = g.release();
+  });
+}
+
+sme_status sme_graph_info(const sme_graph* g, uint64_t* n, uint64_t* m, uint64_t* max_degree) {
+  if (!g) return SME_ERR_INVALID_ARG;
+  if (n) *n = g->g.n;
+  if (m) *m = g->g.m;
+  if (max_degree) *max_degree = g->g.MaxDegree();
+  return SME_OK;
+}
+
+sme_status sme_graph_csr(const sme_graph* g, const uint64_t** row_ptrs, const uint32_t** cols) {
+  if (!g) return SME_ERR_INVALID_ARG;
+  if (row_ptrs) *row_ptrs = g->g.row_ptrs;
+  if (cols) *cols = g->g.cols;
+  return SME_OK;
+}
+
+sme_status sme_graph_write_bin(const sme_graph* g, const char* path) {
+  if (!g || !path) return SME_ERR_INVALID_ARG;
+  return Guard([&] { WriteBinFile(path, g->g); });
+}
+
+sme_status sme_graph_preprocess(sme_graph* g) {
+  if (!g) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    if (g->g.dev) {
+      FreeDeviceGraph(g->g.dev);
+      g->g.dev = nullptr;
+    }
+    Preprocess(g->g);
+  });
+}
+
+sme_status sme_graph_validate(const sme_graph* g) {
+  if (!g) return SME_ERR_INVALID_ARG;
+  return Guard([&] { Validate(g->g); });
+}
+
+sme_status sme_graph_to_device(sme_graph* g, int device) {
+  if (!g) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    if (g->g.dev && g->g.dev->device == device) return;
+    if (g->g.dev) {
+      FreeDeviceGraph(g->g.dev);
+      g->g.dev = nullptr;
+    }
+    if (DeviceCount() <= device) Fail(SME_ERR_NO_DEVICE, "no CUDA device " + std::to_string(device));
+    cudaSetDevice(device);
+    g->g.dev = UploadGraph(g->g, device, 0, nullptr);
+  });
+}
+
+sme_status sme_graph_release_device(sme_graph* g) {
+  if (!g) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    FreeDeviceGraph(g->g.dev);
+    g->g.dev = nullptr;
+  });
+}
+
+sme_status sme_graph_free(sme_graph* g) {
+  if (!g) return SME_OK;
+  return Guard([&] {
+    FreeDeviceGraph(g->g.dev);
+    g->g.dev = nullptr;
+    delete g;
+  });
+}
+
+sme_status sme_generate_rmat(int32_t scale, int32_t ef, double a, double b, double c, uint64_t seed,
+                             sme_graph** out) {
+  if (!out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    std::unique_ptr<sme_graph> g(new sme_graph());
+    GenerateRmat(scale, ef, a, b, c, seed, g->g);
+    *out = g.release();
+  });
+}
+
+sme_status sme_generate_er(uint64_t n, double d, uint64_t seed, sme_graph** out) {
+  if (!out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    std::unique_ptr<sme_graph> g(new sme_graph());
+    GenerateER(n, d, seed, g->g);
+    *out = g.release();
+  });
+}
+
+sme_status sme_generate_ba(uint64_t n, uint32_t m, uint64_t seed, sme_graph** out) {
+  if (!out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    std::unique_ptr<sme_graph> g(new sme_graph());
+    GenerateBA(n, m, seed, g->g);
+    *out = g.release();
+  });
+}
+
+sme_status sme_generate_clique(uint64_t n, sme_graph** out) {
+  if (!out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    std::unique_ptr<sme_graph> g(new sme_graph());
+    GenerateClique(n, g->g);
+    *out = g.release();
+  });
+}
+
+sme_status sme_count(sme_graph* g, const sme_opts* opts, uint64_t* count) {
+  if (!g || !opts || !count) return SME_ERR_INVALID_ARG;
+  return Guard([&] { *count = Execute(g, *opts, false, nullptr, 0).count; });
+}
+
+sme_status sme_enumerate(sme_graph* g, const sme_opts* opts, uint32_t* out, uint64_t cap, uint64_t* n_out) {
+  if (!g || !opts || !n_out || (cap && !out)) return SME_ERR_INVALID_ARG;
+  sme_status st = Guard([&] {
+    RunOut r = Execute(g, *opts, true, out, cap);
+    *n_out = r.emitted;
+  });
+  if (st == SME_OK && *n_out > cap) {
+    SetLastError("enumeration produced " + std::to_string(*n_out) + " instances, buffer holds " +
+                 std::to_string(cap));
+    return SME_ERR_CAPACITY;
+  }
+  return st;
+}
+
+sme_status sme_last_stats(sme_stats* s) {
+  if (!s) return SME_ERR_INVALID_ARG;
+  *s = t_last_stats;
+  return SME_OK;
+}
+
+int32_t sme_query_vertex_count(int32_t q) {
+  if (q < 0 || q >= SME_NUM_QUERIES) return -1;
+  return Query(q).n;
+}
+
+sme_status sme_plan_describe(int32_t q, int32_t plan_type, char* buf, uint64_t cap, uint64_t* needed) {
+  std::string text;
+  sme_status st = Guard([&] {
+    Query query(q);
+    switch (plan_type) {
+      case 0: text = TraversalPlan(query).Describe(); break;
+      case 1: text = ReusePlan(query, true).Describe(); break;
+      case 2: text = LazyPlan(query, SME_COMPRESS_NON_MATERIALIZE_OPT).Describe(); break;
+      case 3: text = ReusePlan(query, false).Describe(); break;
+      case 4: text = LazyPlan(query, SME_COMPRESS_SPECIAL).Describe(); break;
+      case 5: {
+        sme_opts o;
+        sme_opts_default(&o);
+        o.query_type = q;
+        for (int a : {SME_GPU_GPSM, SME_GPU_GPSM_REUSE, SME_GPU_LIGHT}) {
+          o.algo = a;
+          text += Compile(o, false).Describe();
+        }
+        break;
+      }
+      default: Fail(SME_ERR_INVALID_ARG, "plan_type must be 0..5");
+    }
+  });
+  if (st != SME_OK) return st;
+  if (needed) *needed = text.size() + 1;
+  if (!buf || cap < text.size() + 1) return SME_ERR_CAPACITY;
+  std::memcpy(buf, text.c_str(), text.size() + 1);
+  return SME_OK;
+}
+
+const char* sme_last_error(void) { return t_last_error.c_str(); }
+const char* sme_version(void) { return "sme-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

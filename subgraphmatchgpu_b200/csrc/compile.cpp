@@ -1,0 +1,350 @@
+// Compiles a query under one of the three GPU plans into the level program
+// run by the device engine.  One step per reference execute level:
+//
+//   GPU_GPSM        per level: intersect backward lists with the whole-ordered
+//                   conditions, then materialise (Gpsm::JoinPhase,
+//                   src/gpu/impl/gpsm/GPSMCheckConstraints.cuh:40-105).  The
+//                   final level is counted instead of materialised unless
+//                   instances are requested; the count is the same number as
+//                   the size of the last level (IsProcessOver,
+//                   src/gpu/impl/gpsm/HybridGPSMGPUProcessor.cuh:23-33).
+//   GPU_LIGHT       the LIGHT execute sequence, op by op
+//                   (HybridLIGHTGPUProcessor::ExecuteBatch,
+//                   src/gpu/impl/light/HybridLIGHTGPUProcessor.cuh:147-228).
+//   GPU_GPSM_REUSE  per level: when a later level reuses this level's
+//                   intersection, the intersection is computed without the
+//                   ordering conditions and kept as a cache while the level is
+//                   materialised with the conditions (the "intersect-only"
+//                   and "overall" outputs of GpsmReuseBinSearch,
+//                   src/gpu/utils/ops/intersect/GPSMReuseBinSearch.cuh:167-221);
+//                   a reusing level starts from the cached set of its
+//                   ancestor and intersects the separate lists
+//                   (GpsmReuse::JoinPhase, GPSMReuseCheckConstraints.cuh:166-338).
+#include <algorithm>
+#include <sstream>
+
+#include "sme_internal.h"
+
+namespace sme {
+
+namespace {
+std::vector<StepCond> Conds(const std::vector<CondType>& c) {
+  std::vector<StepCond> r;
+  for (auto& x : c) r.push_back(StepCond{(uint8_t)x.first, (uint8_t)x.second});
+  return r;
+}
+std::vector<uint8_t> U8(const std::vector<uintV>& v) {
+  return std::vector<uint8_t>(v.begin(), v.end());
+}
+
+// Tracks which vertices are materialised / hold live candidate sets.
+struct State {
+  std::vector<uint8_t> mat, sets;
+  void AddMat(uint8_t u) { mat.push_back(u); }
+  void AddSet(uint8_t u) {
+    if (std::find(sets.begin(), sets.end(), u) == sets.end()) sets.push_back(u);
+  }
+  void DropSet(uint8_t u) { sets.erase(std::remove(sets.begin(), sets.end(), u), sets.end()); }
+  void Stamp(Step& s) const {
+    s.mat_after = mat;
+    s.sets_after = sets;
+  }
+};
+
+const char* KindName(StepKind k) {
+  switch (k) {
+    case S_INIT: return "INIT";
+    case S_COMPUTE: return "COMPUTE";
+    case S_MATERIALIZE: return "MATERIALIZE";
+    case S_FILTER: return "FILTER_COMPUTE";
+    case S_COMPUTE_COUNT: return "COMPUTE_COUNT";
+    case S_PATH_COUNT: return "COMPUTE_PATH_COUNT";
+    case S_COUNT: return "COUNT";
+  }
+  return "?";
+}
+
+Program CompileGpsm(const Query& q, bool enumerate) {
+  TraversalPlan tp(q);
+  Program p;
+  State st;
+  p.n = q.n;
+  for (int u = 0; u < q.n; ++u) p.out_slot.push_back((uint8_t)u);
+  Step s0;
+  s0.kind = S_INIT;
+  s0.u = 0;
+  st.AddMat(0);
+  st.Stamp(s0);
+  p.steps.push_back(s0);
+  for (int u = 1; u < q.n; ++u) {
+    bool last = u == q.n - 1;
+    Step c;
+    c.kind = (last && !enumerate) ? S_COMPUTE_COUNT : S_COMPUTE;
+    c.u = (uint8_t)u;
+    c.conn = U8(tp.ordered_conn[u]);
+    c.cond = Conds(tp.whole_order[u]);
+    if (c.kind == S_COMPUTE) st.AddSet((uint8_t)u);
+    st.Stamp(c);
+    p.steps.push_back(c);
+    if (c.kind == S_COMPUTE) {
+      Step m;
+      m.kind = S_MATERIALIZE;
+      m.u = (uint8_t)u;
+      st.DropSet((uint8_t)u);
+      st.AddMat((uint8_t)u);
+      st.Stamp(m);
+      p.steps.push_back(m);
+    }
+  }
+  return p;
+}
+
+Program CompileReuse(const Query& q, bool autogen, bool enumerate) {
+  ReusePlan rp(q, autogen);
+  TraversalPlan tp(q);  // only for the helpers; reuse uses relabelled con
+  (void)tp;
+  Program p;
+  State st;
+  const int n = q.n;
+  p.n = n;
+  p.out_slot.resize(n);
+  for (int i = 0; i < n; ++i) p.out_slot[i] = (uint8_t)rp.seq[i];
+  // ordered (backward) connectivity and whole ordering of the relabelled
+  // pattern (DevTraversalPlan built from the relabelled TraversalPlan).
+  AllConnType oc(n);
+  AllCondType wo(n);
+  for (int u = 0; u < n; ++u) {
+    for (uintV v : rp.con[u])
+      if ((int)v < u) oc[u].push_back(v);
+    for (int v = 0; v < u; ++v) wo[u].push_back(CondType(GetConditionType(u, v, rp.order), (uintV)v));
+  }
+  Step s0;
+  s0.kind = S_INIT;
+  s0.u = 0;
+  st.AddMat(0);
+  st.Stamp(s0);
+  p.steps.push_back(s0);
+  for (int u = 1; u < n; ++u) {
+    const VertexReusePlan& vp = rp.levels[u];
+    bool last = u == n - 1;
+    Step c;
+    c.u = (uint8_t)u;
+    c.full_conn = U8(oc[u]);
+    // Reuse one ancestor cache (identity mapping on the prefix); any other
+    // reuse meta is intersected from its adjacency lists instead.
+    std::vector<uint8_t> conn = U8(vp.separate);
+    int src = -1;
+    for (auto& r : vp.reuse) {
+      bool ancestor = r.source_vertex < (uintV)u && r.mapping.size() == (size_t)n &&
+                      r.mapping[r.source_vertex] == (uintV)u;
+      for (uintV x = 0; ancestor && x < r.source_vertex; ++x)
+        if (r.mapping[x] != x) ancestor = false;
+      if (ancestor && src < 0 && rp.cache_required[r.source_vertex]) {
+        src = (int)r.source_vertex;
+      } else {
+        for (uintV x : r.conn) conn.push_back((uint8_t)x);
+      }
+    }
+    std::sort(conn.begin(), conn.end());
+    conn.erase(std::unique(conn.begin(), conn.end()), conn.end());
+    c.conn = conn;
+    c.reuse_src = (int8_t)src;
+    if (rp.cache_required[u] && !last) {
+      // intersect-only result kept as the cache; conditions at materialise
+      c.kind = S_COMPUTE;
+      st.AddSet((uint8_t)u);
+      st.Stamp(c);
+      p.steps.push_back(c);
+      Step m;
+      m.kind = S_MATERIALIZE;
+      m.u = (uint8_t)u;
+      m.cond = Conds(wo[u]);
+      m.keep_set = true;
+      st.AddMat((uint8_t)u);
+      st.Stamp(m);
+      p.steps.push_back(m);
+    } else {
+      c.kind = (last && !enumerate) ? S_COMPUTE_COUNT : S_COMPUTE;
+      c.cond = Conds(wo[u]);
+      if (c.kind == S_COMPUTE) st.AddSet((uint8_t)u);
+      st.Stamp(c);
+      p.steps.push_back(c);
+      if (c.kind == S_COMPUTE) {
+        Step m;
+        m.kind = S_MATERIALIZE;
+        m.u = (uint8_t)u;
+        st.DropSet((uint8_t)u);
+        st.AddMat((uint8_t)u);
+        st.Stamp(m);
+        p.steps.push_back(m);
+      }
+    }
+    // caches no longer referenced by a later level are dropped
+    for (uint8_t s : std::vector<uint8_t>(st.sets)) {
+      bool used = false;
+      for (int k = u + 1; k < n; ++k)
+        for (auto& r : rp.levels[k].reuse)
+          if (r.source_vertex == s) used = true;
+      if (!used) {
+        st.DropSet(s);
+        p.steps.back().sets_after = st.sets;
+      }
+    }
+  }
+  return p;
+}
+
+// LIGHT: the reference execute sequence; for enumeration the counting tail
+// is replaced by materialising every vertex (conditions recomputed by the
+// same utilities, so each pair of pattern vertices is still checked once).
+Program CompileLight(const Query& q, int compress_level, bool enumerate) {
+  LazyPlan lp(q, compress_level);
+  if (enumerate) {
+    std::vector<LazyEntry> e;
+    for (auto x : lp.exec) {
+      if (x.first == L_COUNT) continue;
+      if (x.first == L_COMPUTE_COUNT || x.first == L_COMPUTE_PATH_COUNT) x.first = L_COMPUTE;
+      e.push_back(x);
+    }
+    std::vector<bool> mat(q.n, false);
+    for (auto& x : e)
+      if (x.first == L_MATERIALIZE) mat[x.second] = true;
+    for (auto& x : std::vector<LazyEntry>(e))
+      if (x.first == L_COMPUTE && !mat[x.second]) {
+        e.push_back(LazyEntry(L_MATERIALIZE, x.second));
+        mat[x.second] = true;
+      }
+    lp.exec = e;
+    // recompute per-level sets and conditions for the new sequence
+    LazyPlan fresh(q, compress_level);
+    fresh.exec = e;
+    LightConstraintsFor(fresh);
+    lp = fresh;
+  }
+  Program p;
+  State st;
+  p.n = q.n;
+  for (int u = 0; u < q.n; ++u) p.out_slot.push_back((uint8_t)u);
+  const bool direct_ok = lp.compress_level == SME_COMPRESS_SPECIAL && q.type <= 11 && q.type != 4 &&
+                         q.type != 9;  // CanDirectCount, LIGHTDirectCount.cuh:13-19
+  for (size_t i = 0; i < lp.exec.size(); ++i) {
+    LazyOp op = lp.exec[i].first;
+    uint8_t u = (uint8_t)lp.exec[i].second;
+    Step s;
+    s.u = u;
+    switch (op) {
+      case L_MATERIALIZE:
+        if (i == 0) {
+          s.kind = S_INIT;
+        } else {
+          s.kind = S_MATERIALIZE;
+          s.cond = Conds(lp.materialize_cond[u]);
+          st.DropSet(u);
+        }
+        st.AddMat(u);
+        break;
+      case L_COMPUTE:
+      case L_COMPUTE_PATH_COUNT:
+        s.kind = op == L_COMPUTE ? S_COMPUTE : S_PATH_COUNT;
+        s.conn = U8(lp.backward_conn[u]);
+        s.cond = Conds(lp.compute_cond[u]);
+        st.AddSet(u);
+        break;
+      case L_FILTER_COMPUTE:
+        s.kind = S_FILTER;
+        s.cond = Conds(lp.filter_cond[u]);
+        break;
+      case L_COMPUTE_COUNT: {
+        s.kind = S_COMPUTE_COUNT;
+        s.conn = U8(lp.backward_conn[u]);
+        s.cond = Conds(lp.compute_cond[u]);
+        auto& um = lp.computed_unmaterialized[i];
+        if (um.size() > 1) Fail(SME_ERR_UNSUPPORTED_QUERY, "COMPUTE_COUNT with >1 unmaterialized vertex");
+        if (um.size() == 1) {
+          s.with_u = (int8_t)um[0];
+          s.with_op = (uint8_t)GetConditionType(u, um[0], q.order);
+        }
+        break;
+      }
+      case L_COUNT: {
+        s.kind = S_COUNT;
+        s.unmat = U8(lp.computed_unmaterialized[i]);
+        s.direct = direct_ok;
+        if (!s.direct && s.unmat.size() == 2)
+          s.pair_op = (uint8_t)GetConditionType(s.unmat[0], s.unmat[1], q.order);
+        if (!s.direct && (s.unmat.empty() || s.unmat.size() > 2))
+          Fail(SME_ERR_UNSUPPORTED_QUERY, "COUNT over " + std::to_string(s.unmat.size()) +
+                                              " unmaterialized vertices");
+        break;
+      }
+    }
+    st.Stamp(s);
+    p.steps.push_back(s);
+  }
+  return p;
+}
+}  // namespace
+
+Program Compile(const sme_opts& o, bool enumerate) {
+  Query q(o.query_type, o.enable_ordering != 0);
+  Program p;
+  switch (o.algo) {
+    case SME_GPU_GPSM:
+      p = CompileGpsm(q, enumerate);
+      break;
+    case SME_GPU_GPSM_REUSE: {
+      bool autogen = o.reuse_autogen == 1 || (o.reuse_autogen < 0 && !HasHardcodedReusePlan(q.type));
+      p = CompileReuse(q, autogen, enumerate);
+      break;
+    }
+    case SME_GPU_LIGHT:
+      if (o.compress_level < 0 || o.compress_level > 3)
+        Fail(SME_ERR_INVALID_ARG, "compress_level must be 0..3");
+      p = CompileLight(q, o.compress_level, enumerate);
+      break;
+    default:
+      Fail(SME_ERR_INVALID_ARG, "algo must be 4 (GPU_GPSM), 5 (GPU_GPSM_REUSE) or 6 (GPU_LIGHT)");
+  }
+  p.query_type = q.type;
+  p.algo = o.algo;
+  p.enumerate = enumerate;
+  for (auto& s : p.steps) {
+    std::ostringstream os;
+    os << KindName(s.kind) << "(" << (int)s.u << ")";
+    s.label = os.str();
+  }
+  return p;
+}
+
+std::string Program::Describe() const {
+  std::ostringstream os;
+  os << "program Q" << query_type << " algo=" << algo << (enumerate ? " enumerate" : " count") << "\n";
+  for (size_t i = 0; i < steps.size(); ++i) {
+    const Step& s = steps[i];
+    os << i << ": " << s.label;
+    if (!s.conn.empty()) {
+      os << " conn=(";
+      for (size_t j = 0; j < s.conn.size(); ++j) os << (j ? "," : "") << (int)s.conn[j];
+      os << ")";
+    }
+    if (s.reuse_src >= 0) os << " reuse=" << (int)s.reuse_src;
+    if (!s.cond.empty()) {
+      os << " cond=(";
+      for (size_t j = 0; j < s.cond.size(); ++j)
+        os << (j ? "," : "") << (s.cond[j].op == 0 ? "<" : s.cond[j].op == 1 ? ">" : "!=")
+           << (int)s.cond[j].operand;
+      os << ")";
+    }
+    if (s.with_u >= 0) os << " with=" << (int)s.with_u;
+    if (s.kind == S_COUNT) os << (s.direct ? " direct" : " general");
+    if (s.keep_set) os << " keep";
+    os << " | mat=(";
+    for (size_t j = 0; j < s.mat_after.size(); ++j) os << (j ? "," : "") << (int)s.mat_after[j];
+    os << ") sets=(";
+    for (size_t j = 0; j < s.sets_after.size(); ++j) os << (j ? "," : "") << (int)s.sets_after[j];
+    os << ")\n";
+  }
+  return os.str();
+}
+
+}  // namespace sme

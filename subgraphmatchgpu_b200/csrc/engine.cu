@@ -1,0 +1,975 @@
+// Device engine: level-by-level extension of partial instances with
+// memory-bounded batches, depth first over batches.
+//
+// Host control mirrors HybridGPUProcessor::ProcessLevel
+// (src/gpu/impl/common/HybridGPUProcessor.cuh:14-50): per level, estimate each
+// path's output (children estimate), split the frontier into batches that fit
+// the level's memory budget (BatchManager::OrganizeBatch,
+// src/gpu/utils/batch/BatchManager.cuh:42-110), execute the batch, recurse.
+// Differences by design:
+//   * one device allocation per context, used as a LIFO stack (no allocator
+//     calls in the loop; the reference uses cnmem + per-op DeviceArray);
+//   * intersections write in a single pass into a gapped buffer sized by the
+//     children estimate, instead of count pass + scan + DToH + write pass
+//     (GpsmBinSearch, src/gpu/utils/ops/intersect/GPSMBinSearch.cuh:144-197);
+//   * candidate sets are (pointer, count) views: a set that is a sub-range of
+//     an adjacency list or of an earlier set is not copied;
+//   * counts accumulate on the device; the host reads one uint64 at the end.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <string>
+
+#include "engine.h"
+#include "kernels.cuh"
+
+namespace sme {
+
+using namespace dev;
+
+#define CK(x)                                                                            \
+  do {                                                                                   \
+    cudaError_t e_ = (x);                                                                \
+    if (e_ != cudaSuccess) Fail(SME_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---------------------------------------------------------------- kernels --
+namespace {
+
+__global__ void k_iota(uint32_t* out, uint32_t n, uint32_t start) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = start + i;
+}
+
+// Children estimate of an intersection step: the smallest list (the pivot
+// size), an upper bound of the candidate count (ThreadEstimatePathCount<MIN>,
+// CheckConstraintsCommon.cuh:161-189).
+__global__ void k_est_compute(DFront F, DStep s, const uintE* __restrict__ rp, uint64_t* est) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x) {
+    uint64_t m = ~0ULL;
+    for (int i = 0; i < s.nconn; ++i) {
+      uint32_t v = F.inst[s.conn[i]][p];
+      m = min(m, (uint64_t)(rp[v + 1] - rp[v]));
+    }
+    if (s.reuse >= 0) {
+      const uint32_t* ptr;
+      uint32_t len;
+      GetSet(F, s.reuse, p, ptr, len);
+      m = min(m, (uint64_t)len);
+    }
+    est[p] = m == ~0ULL ? 0 : m;
+  }
+}
+
+__global__ void k_est_set(DFront F, int u, uint64_t* est) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x) {
+    uint32_t s = SetIndex(F, u, p);
+    est[p] = F.set[u].cnt[s];
+  }
+}
+
+// ---- inclusive scan of uint64 (tile 4096 = 512 threads x 8) -------------
+constexpr int SCAN_THREADS = 512;
+constexpr int SCAN_ITEMS = 8;
+constexpr uint32_t SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ uint64_t BlockExclusiveScan(uint64_t v, uint64_t* total) {
+  __shared__ uint64_t warp_tot[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    uint64_t t = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t y = __shfl_up_sync(FULL, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < nw) warp_tot[lane] = t;
+  }
+  __syncthreads();
+  uint64_t warp_prefix = wid > 0 ? warp_tot[wid - 1] : 0;
+  uint64_t excl = warp_prefix + x - v;
+  if (total) *total = warp_tot[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return excl;
+}
+
+__global__ void k_scan_reduce(const uint64_t* __restrict__ in, uint32_t n, uint64_t* bs) {
+  uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+  uint64_t s = 0;
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    uint64_t i = base + (uint64_t)k * SCAN_THREADS + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  __shared__ uint64_t red[SCAN_THREADS / 32];
+  s = WarpSum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint64_t t = threadIdx.x < SCAN_THREADS / 32 ? red[threadIdx.x] : 0;
+    t = WarpSum(t);
+    if (threadIdx.x == 0) bs[blockIdx.x] = t;
+  }
+}
+
+// Exclusive scan of the block sums in place (one block).
+__global__ void k_scan_partials(uint64_t* bs, uint32_t nb) {
+  uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+  uint32_t b = threadIdx.x * per, e = min(nb, b + per);
+  uint64_t s = 0;
+  for (uint32_t i = b; i < e; ++i) s += bs[i];
+  uint64_t run = BlockExclusiveScan(s, nullptr);
+  for (uint32_t i = b; i < e; ++i) {
+    uint64_t v = bs[i];
+    bs[i] = run;
+    run += v;
+  }
+}
+
+__global__ void k_scan_apply(uint64_t* data, uint32_t n, const uint64_t* __restrict__ bs) {
+  uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+  uint64_t v[SCAN_ITEMS];
+  uint64_t s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    uint64_t i = base + k;
+    v[k] = i < n ? data[i] : 0;
+    s += v[k];
+  }
+  uint64_t run = BlockExclusiveScan(s, nullptr) + bs[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    uint64_t i = base + k;
+    run += v[k];
+    if (i < n) data[i] = run;
+  }
+}
+
+// Batch boundaries: for threshold k, the first path whose inclusive cost
+// exceeds cost(start-1) + (k+1)*budget (SplitBatchKernel,
+// src/gpu/utils/batch/SplitBatch.cuh:38-87).  cost(p) = pf*(p+1) + cf*est_incl[p].
+__global__ void k_split(const uint64_t* __restrict__ incl, uint32_t P, uint32_t start, double pf,
+                        double cf, double budget, uint32_t K, uint64_t* out) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  double c0 = start == 0 ? 0.0 : pf * (double)start + cf * (double)incl[start - 1];
+  double t = c0 + (double)(k + 1) * budget;
+  uint32_t lo = start, hi = P;  // first p in [start,P) with cost(p) > t
+  while (lo < hi) {
+    uint32_t mid = lo + (hi - lo) / 2;
+    double c = pf * (double)(mid + 1) + cf * (double)incl[mid];
+    if (c > t) hi = mid;
+    else lo = mid + 1;
+  }
+  out[2 * k] = lo;
+  out[2 * k + 1] = lo == 0 ? 0 : incl[lo - 1];
+  if (lo == start) {  // a single path above the budget: its own batch
+    out[2 * k] = start + 1;
+    out[2 * k + 1] = incl[start];
+  }
+}
+
+// ---- intersection (COMPUTE / COMPUTE_COUNT / COMPUTE_PATH_COUNT) ---------
+// One warp per path.  The pivot is the smallest list (ThreadChoosePivotLevel,
+// CheckConstraintsCommon.cuh:10-29); < and > conditions clip the pivot to a
+// sub-range by binary search before the scan; every pivot element is checked
+// in the other lists by a per-lane binary search whose lower end advances with
+// the lane's previous hit (each lane sees increasing candidates).
+// MODE 0 writes the sorted candidate set, MODE 1 counts (optionally ranked
+// into a partner set), MODE 2 stores only the per-path count.
+template <int MODE>
+__global__ void __launch_bounds__(WARP_BLOCK) k_compute(
+    DFront F, DStep s, const uintE* __restrict__ rp, const uint32_t* __restrict__ cols,
+    const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr, uint32_t* out_cnt,
+    uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const unsigned lt = (1u << lane) - 1;
+  unsigned long long local = 0, bytes = 0;
+  const uint64_t base = b0 == 0 ? 0 : est_incl[b0 - 1];
+
+  for (uint32_t p = gw; p < F.P; p += nw) {
+    const uint32_t* L[MAXV];
+    uint32_t N[MAXV];
+    int nl = 0;
+#pragma unroll
+    for (int i = 0; i < MAXV; ++i) {
+      if (i < s.nconn) {
+        uint32_t v = F.inst[s.conn[i]][p];
+        uintE b = rp[v], e = rp[v + 1];
+        L[i] = cols + b;
+        N[i] = (uint32_t)(e - b);
+        nl = i + 1;
+      }
+    }
+    if (s.reuse >= 0) {
+#pragma unroll
+      for (int i = 0; i < MAXV; ++i)
+        if (i == nl) GetSet(F, s.reuse, p, L[i], N[i]);
+      ++nl;
+    }
+    if (lane == 0) {
+      uint64_t b = 12ULL * s.nconn;
+#pragma unroll
+      for (int i = 0; i < MAXV; ++i)
+        if (i < nl) b += 4ULL * N[i];
+      bytes += b;
+    }
+    // pivot to slot 0
+#pragma unroll
+    for (int i = 1; i < MAXV; ++i) {
+      if (i < nl && N[i] < N[0]) {
+        const uint32_t* tp = L[0];
+        L[0] = L[i];
+        L[i] = tp;
+        uint32_t tn = N[0];
+        N[0] = N[i];
+        N[i] = tn;
+      }
+    }
+    Bounds bd = MakeBounds(s.cond, F, p);
+    uint32_t r0 = 0, r1 = 0;
+    if (nl > 0) Range(L[0], N[0], bd, r0, r1);
+
+    uint64_t out_off = 0;
+    if (MODE == 0) {
+      out_off = (p + b0 == 0 ? 0 : est_incl[p + b0 - 1]) - base;
+      if (nl == 1) {
+        // single list: the candidate set is a sub-range unless an excluded
+        // value falls inside it
+        uint32_t ex[MAXV];
+        int ne = Exclusions(L[0], r0, r1, bd, ex);
+        if (ne == 0) {
+          if (lane == 0) {
+            out_ptr[p] = (uint64_t)(L[0] + r0);
+            out_cnt[p] = r1 - r0;
+            bytes += 4ULL * (r1 - r0);
+          }
+          continue;
+        }
+      }
+    }
+    // partner set for ranked counting
+    const uint32_t* W = nullptr;
+    uint32_t WN = 0;
+    if (MODE == 1 && s.with_u >= 0) GetSet(F, s.with_u, p, W, WN);
+
+    uint32_t cur[MAXV];
+#pragma unroll
+    for (int i = 0; i < MAXV; ++i) cur[i] = 0;
+    uint32_t written = 0;
+    for (uint32_t bi = r0; bi < r1; bi += 32) {
+      uint32_t i = bi + lane;
+      bool ok = i < r1;
+      uint32_t x = ok ? __ldg(L[0] + i) : 0;
+#pragma unroll
+      for (int k = 0; k < MAXV; ++k)
+        if (k < bd.nne && x == bd.ne[k]) ok = false;
+#pragma unroll
+      for (int j = 1; j < MAXV; ++j) {
+        if (j < nl && ok) {
+          uint32_t pos = cur[j] + LowerBound(L[j] + cur[j], N[j] - cur[j], x);
+          cur[j] = pos;
+          ok = pos < N[j] && __ldg(L[j] + pos) == x;
+        }
+      }
+      unsigned mask = __ballot_sync(FULL, ok);
+      if (MODE == 0) {
+        uint64_t o = out_off + written + __popc(mask & lt);
+        if (ok) {
+          if (o < out_cap) out_data[o] = x;
+          else atomicOr(err, ENGINE_ERR_BOUNDS);
+        }
+      } else if (MODE == 1) {
+        if (W != nullptr) {
+          if (ok) local += RankCount(W, WN, x, s.with_op);
+        } else if (lane == 0) {
+          local += __popc(mask);
+        }
+      }
+      written += __popc(mask);
+    }
+    if (lane == 0) {
+      if (MODE == 0) {
+        out_ptr[p] = (uint64_t)(out_data + out_off);
+        out_cnt[p] = written;
+        bytes += 4ULL * written;
+      } else if (MODE == 2) {
+        out_ptr[p] = 0;
+        out_cnt[p] = written;
+      }
+    }
+  }
+  if (MODE == 1) {
+    local = WarpSum(local);
+    if (lane == 0 && local) atomicAdd(acc, local);
+  }
+  if (lane == 0 && bytes) atomicAdd(acc + 1, bytes);
+}
+
+// ---- MATERIALIZE ---------------------------------------------------------
+// Valid children per path: set range clipped by < / >, minus excluded values.
+__global__ void k_mat_count(DFront F, int u, DCond c, uint64_t* cnt) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x) {
+    const uint32_t* a;
+    uint32_t n;
+    GetSet(F, u, p, a, n);
+    Bounds bd = MakeBounds(c, F, p);
+    uint32_t r0, r1, ex[MAXV];
+    Range(a, n, bd, r0, r1);
+    int ne = Exclusions(a, r0, r1, bd, ex);
+    cnt[p] = (uint64_t)(r1 - r0 - ne);
+  }
+}
+
+// Expands each path's valid candidates into child rows: materialised columns
+// (broadcast from the parent) plus the new vertex, and the set index of every
+// live candidate set (Materialize, src/gpu/impl/light/op/LIGHTMaterialize.cuh:23-162,
+// fused: expand + filter + compact + per-column gather in one pass).
+__global__ void __launch_bounds__(WARP_BLOCK) k_mat_write(DFront F, DCond c, DMatOut o,
+                                                          const uint64_t* __restrict__ incl,
+                                                          uint64_t total, uint32_t* err) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const int u = o.u;
+  for (uint32_t p = gw; p < F.P; p += nw) {
+    const uint32_t* a;
+    uint32_t n;
+    GetSet(F, u, p, a, n);
+    Bounds bd = MakeBounds(c, F, p);
+    uint32_t r0, r1, ex[MAXV];
+    Range(a, n, bd, r0, r1);
+    int ne = Exclusions(a, r0, r1, bd, ex);
+    uint64_t off = (p == 0 ? 0 : incl[p - 1]);
+    uint32_t vals[MAXV], idx[MAXV];
+#pragma unroll
+    for (int i = 0; i < MAXV; ++i) {
+      vals[i] = 0;
+      idx[i] = 0;
+      if (i < o.nmat && o.mat[i] != u) vals[i] = F.inst[o.mat[i]][p];
+      if (i < o.nsets) idx[i] = SetIndex(F, o.sets[i], p);
+    }
+    for (uint32_t j = r0 + lane; j < r1; j += 32) {
+      int before = 0;
+      bool skip = false;
+#pragma unroll
+      for (int k = 0; k < MAXV; ++k) {
+        if (k < ne) {
+          if (ex[k] == j) skip = true;
+          if (ex[k] < j) ++before;
+        }
+      }
+      if (skip) continue;
+      uint64_t w = off + (j - r0) - before;
+      if (w >= total) {
+        atomicOr(err, ENGINE_ERR_BOUNDS);
+        continue;
+      }
+      uint32_t x = __ldg(a + j);
+#pragma unroll
+      for (int i = 0; i < MAXV; ++i) {
+        if (i < o.nmat) o.inst[o.mat[i]][w] = o.mat[i] == u ? x : vals[i];
+        if (i < o.nsets) o.cidx[o.sets[i]][w] = idx[i];
+      }
+    }
+  }
+}
+
+// ---- FILTER_COMPUTE ------------------------------------------------------
+// Re-applies conditions to a computed set (FilterCandidate,
+// src/gpu/impl/light/op/LIGHTFilterCompute.cuh:22-155).  A filtered set with
+// no excluded value inside its range is a view of the old set.
+__global__ void __launch_bounds__(WARP_BLOCK) k_filter(DFront F, int u, DCond c,
+                                                       const uint64_t* __restrict__ est_incl, uint32_t b0,
+                                                       uint64_t* out_ptr, uint32_t* out_cnt,
+                                                       uint32_t* out_data, uint64_t out_cap, uint32_t* err) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint64_t base = b0 == 0 ? 0 : est_incl[b0 - 1];
+  for (uint32_t p = gw; p < F.P; p += nw) {
+    const uint32_t* a;
+    uint32_t n;
+    GetSet(F, u, p, a, n);
+    Bounds bd = MakeBounds(c, F, p);
+    uint32_t r0, r1, ex[MAXV];
+    Range(a, n, bd, r0, r1);
+    int ne = Exclusions(a, r0, r1, bd, ex);
+    if (ne == 0) {
+      if (lane == 0) {
+        out_ptr[p] = (uint64_t)(a + r0);
+        out_cnt[p] = r1 - r0;
+      }
+      continue;
+    }
+    uint64_t off = (p + b0 == 0 ? 0 : est_incl[p + b0 - 1]) - base;
+    for (uint32_t j = r0 + lane; j < r1; j += 32) {
+      int before = 0;
+      bool skip = false;
+      for (int k = 0; k < ne; ++k) {
+        if (ex[k] == j) skip = true;
+        if (ex[k] < j) ++before;
+      }
+      if (skip) continue;
+      uint64_t w = off + (j - r0) - before;
+      if (w < out_cap) out_data[w] = __ldg(a + j);
+      else atomicOr(err, ENGINE_ERR_BOUNDS);
+    }
+    if (lane == 0) {
+      out_ptr[p] = (uint64_t)(out_data + off);
+      out_cnt[p] = r1 - r0 - ne;
+    }
+  }
+}
+
+// ---- COUNT (LIGHTCount / LIGHTDirectCount) -------------------------------
+// One unmaterialised vertex: sum of set sizes.
+__global__ void k_count1(DFront F, int u, unsigned long long* acc) {
+  unsigned long long s = 0;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x)
+    s += F.set[u].cnt[SetIndex(F, u, p)];
+  s = WarpSum(s);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
+}
+
+// Two unmaterialised vertices u0,u1 with condition (x0 op x1): each element of
+// the smaller set is ranked in the larger one
+// (GeneralCountTwoComputedVertices, src/gpu/impl/light/op/LIGHTCount.cuh:22-116).
+__global__ void __launch_bounds__(WARP_BLOCK) k_count2(DFront F, int u0, int u1, uint8_t op,
+                                                       unsigned long long* acc) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long s = 0;
+  for (uint32_t p = gw; p < F.P; p += nw) {
+    const uint32_t *A, *B;
+    uint32_t na, nb;
+    GetSet(F, u0, p, A, na);
+    GetSet(F, u1, p, B, nb);
+    if (na <= nb) {
+      for (uint32_t i = lane; i < na; i += 32) s += RankCount(B, nb, __ldg(A + i), op);
+    } else {
+      // count x in A with (x op y) for each y in B
+      uint8_t rop = op == 0 ? 1 : (op == 1 ? 0 : 2);
+      for (uint32_t i = lane; i < nb; i += 32) s += RankCount(A, na, __ldg(B + i), rop);
+    }
+  }
+  s = WarpSum(s);
+  if (lane == 0 && s) atomicAdd(acc, s);
+}
+
+// Closed forms over candidate-set sizes (ThreadDirectCount,
+// src/gpu/impl/light/op/LIGHTDirectCount.cuh:21-79).
+__device__ unsigned long long DirectCount(const unsigned long long* c, int q) {
+  unsigned long long r = 0;
+  switch (q) {
+    case 0: r = c[2]; break;
+    case 1: r = c[3]; break;
+    case 2: r = c[1] > 0 ? c[1] * (c[1] - 1) / 2 : 0; break;
+    case 3: r = c[3]; break;
+    case 5:
+      r = c[1] * c[3] * c[5];
+      if (r > 0) r = r - c[3] * (c[1] - 1 + c[5] - 1) - c[3] * c[3];
+      break;
+    case 6:
+      if (c[4] > 0 && c[2] > 0) r = c[4] * c[2] - c[2];
+      break;
+    case 7: r = c[4]; break;
+    case 8: r = c[4]; break;
+    case 10: r = c[2] > 0 ? c[2] * (c[2] - 1) / 2 : 0; break;
+    case 11: r = c[5]; break;
+    default: r = 0;
+  }
+  return r;
+}
+
+__global__ void k_count_direct(DFront F, uint8_t nu, uint8_t u0, uint8_t u1, uint8_t u2, int q,
+                               unsigned long long* acc) {
+  unsigned long long s = 0;
+  const uint8_t us[3] = {u0, u1, u2};
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x) {
+    unsigned long long c[MAXV] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < nu; ++i) c[us[i]] = F.set[us[i]].cnt[SetIndex(F, us[i], p)];
+    s += DirectCount(c, q);
+  }
+  s = WarpSum(s);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
+}
+
+// Writes complete instances (all vertices materialised), in output slots.
+__global__ void k_emit(DFront F, uint8_t n, const uint8_t* __restrict__ slot_dummy, uint8_t s0,
+                       uint8_t s1, uint8_t s2, uint8_t s3, uint8_t s4, uint8_t s5, uint32_t* out,
+                       uint64_t cap, unsigned long long* counter) {
+  const uint8_t slot[MAXV] = {s0, s1, s2, s3, s4, s5};
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x) {
+    unsigned long long pos = atomicAdd(counter, 1ULL);
+    if (pos < cap)
+      for (int v = 0; v < n; ++v) out[pos * n + slot[v]] = F.inst[v][p];
+  }
+  (void)slot_dummy;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- runtime --
+void* Arena::Alloc(size_t bytes) {
+  size_t b = (bytes + 255) & ~size_t(255);
+  if (b > cap - top)
+    Fail(SME_ERR_OOM, "device arena exhausted: need " + std::to_string(b) + " bytes, " +
+                          std::to_string(cap - top) + " free of " + std::to_string(cap));
+  void* p = base + top;
+  top += b;
+  peak = std::max(peak, top);
+  return p;
+}
+
+int DeviceCount() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+DeviceContext::~DeviceContext() {}
+
+DeviceContext* CreateContext(int device, uint64_t bytes) {
+  if (DeviceCount() <= device || device < 0) Fail(SME_ERR_NO_DEVICE, "no CUDA device " + std::to_string(device));
+  CK(cudaSetDevice(device));
+  auto* c = new DeviceContext();
+  c->device = device;
+  try {
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    uint64_t want = bytes ? bytes : (uint64_t)(fr * 0.80);
+    if (want > fr) want = (uint64_t)(fr * 0.95);
+    CK(cudaMalloc((void**)&c->arena.base, want));
+    c->arena.cap = want;
+    c->pinned_words = 1 << 14;
+    CK(cudaMallocHost((void**)&c->h_pinned, c->pinned_words * sizeof(uint64_t)));
+  } catch (...) {
+    DestroyContext(c);
+    throw;
+  }
+  return c;
+}
+
+void DestroyContext(DeviceContext* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->arena.base) cudaFree(c->arena.base);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, uint64_t* h2d) {
+  CK(cudaSetDevice(device));
+  auto* d = new DeviceGraph();
+  d->device = device;
+  d->n = g.n;
+  d->m = g.m;
+  try {
+    CK(cudaMalloc((void**)&d->row_ptrs, (g.n + 1) * sizeof(uintE)));
+    CK(cudaMalloc((void**)&d->cols, std::max<uint64_t>(g.m, 1) * sizeof(uintV)));
+    CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, stream));
+    if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  } catch (...) {
+    FreeDeviceGraph(d);
+    throw;
+  }
+  if (h2d) *h2d += (g.n + 1) * sizeof(uintE) + g.m * sizeof(uintV);
+  return d;
+}
+
+void FreeDeviceGraph(DeviceGraph* d) {
+  if (!d) return;
+  cudaSetDevice(d->device);
+  if (d->host_mapped) {
+    if (d->row_ptrs) cudaFree(d->row_ptrs);
+  } else {
+    if (d->row_ptrs) cudaFree(d->row_ptrs);
+    if (d->cols) cudaFree(d->cols);
+  }
+  delete d;
+}
+
+// --------------------------------------------------------------- executor --
+namespace {
+
+int SmCount(int device) {
+  static int cached[64] = {0};
+  if (device >= 0 && device < 64 && cached[device]) return cached[device];
+  int v = 148;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+  if (device >= 0 && device < 64) cached[device] = v;
+  return v;
+}
+
+DCond ToDCond(const std::vector<StepCond>& c) {
+  DCond d{};
+  d.n = (uint8_t)c.size();
+  for (size_t i = 0; i < c.size(); ++i) {
+    d.op[i] = c[i].op;
+    d.operand[i] = c[i].operand;
+  }
+  return d;
+}
+
+DStep ToDStep(const Step& s) {
+  DStep d{};
+  d.u = s.u;
+  d.nconn = (uint8_t)s.conn.size();
+  for (size_t i = 0; i < s.conn.size(); ++i) d.conn[i] = s.conn[i];
+  d.reuse = s.reuse_src;
+  d.cond = ToDCond(s.cond);
+  d.with_u = s.with_u;
+  d.with_op = s.with_op;
+  return d;
+}
+
+class Executor {
+ public:
+  Executor(const Program& prog, const DeviceGraph& g, DeviceContext& ctx, uint32_t* d_out, uint64_t cap)
+      : prog_(prog), g_(g), ctx_(ctx), A_(ctx.arena), st_(ctx.stream), out_(d_out), cap_(cap) {
+    sms_ = SmCount(ctx.device);
+  }
+
+  RunResult Run(uint64_t rb, uint64_t re) {
+    auto t0 = std::chrono::steady_clock::now();
+    size_t mark = A_.Mark();
+    ctrl_ = (unsigned long long*)A_.Alloc(8 * sizeof(unsigned long long));
+    CK(cudaMemsetAsync(ctrl_, 0, 8 * sizeof(unsigned long long), st_));
+    const Step& s0 = prog_.steps[0];
+    const uint64_t R = re > rb ? re - rb : 0;
+    // roots: inst column + next level estimate + scan temporaries
+    const uint64_t per_root = 4 + 8 + 8;
+    uint64_t chunk = std::max<uint64_t>(1, Budget(0) / per_root);
+    chunk = std::min<uint64_t>(chunk, 0x7fffffffULL);
+    for (uint64_t b = rb; b < re; b += chunk) {
+      uint32_t P = (uint32_t)std::min<uint64_t>(chunk, re - b);
+      size_t m = A_.Mark();
+      uint32_t* col = (uint32_t*)A_.Alloc((size_t)P * 4);
+      k_iota<<<Grid(P, 256), 256, 0, st_>>>(col, P, (uint32_t)b);
+      Launched();
+      DFront F{};
+      F.P = P;
+      F.inst[s0.u] = col;
+      ++batches_;
+      Level(1, F);
+      A_.Release(m);
+    }
+    (void)R;
+    unsigned long long h[8];
+    CK(cudaMemcpyAsync(h, ctrl_, sizeof(h), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    CK(cudaGetLastError());
+    if (h[3]) Fail(SME_ERR_CUDA, "device bounds check failed (engine error flags " + std::to_string(h[3]) + ")");
+    RunResult r;
+    r.count = prog_.enumerate ? h[2] : h[0];
+    r.emitted = h[2];
+    r.stats.algorithmic_bytes = h[1];
+    r.stats.kernel_launches = launches_;
+    r.stats.batches = batches_;
+    r.stats.peak_device_bytes = A_.peak;
+    r.stats.paths_processed = paths_;
+    float ms_total = 0;
+    for (auto& e : events_) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e.first, e.second);
+      ms_total += ms;
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    events_.clear();
+    r.stats.kernel_ms = ms_total;
+    r.stats.elapsed_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    A_.Release(mark);
+    return r;
+  }
+
+ private:
+  const Program& prog_;
+  const DeviceGraph& g_;
+  DeviceContext& ctx_;
+  Arena& A_;
+  cudaStream_t st_;
+  uint32_t* out_;
+  uint64_t cap_;
+  int sms_ = 148;
+  unsigned long long* ctrl_ = nullptr;  // [0] count [1] bytes [2] emitted [3] error flags
+  uint64_t launches_ = 0, batches_ = 0, paths_ = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events_;
+
+  void Launched() { ++launches_; }
+
+  unsigned Grid(uint64_t items, int per_block) const {
+    uint64_t b = (items + per_block - 1) / per_block;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)sms_ * 16));
+  }
+  unsigned WarpGrid(uint64_t paths) const { return Grid(paths * 32, WARP_BLOCK); }
+
+  uint64_t Budget(size_t k) const {
+    size_t rem = prog_.steps.size() - k + 1;
+    return (uint64_t)((double)A_.Free() * 0.85 / (double)rem);
+  }
+
+  std::pair<cudaEvent_t, cudaEvent_t> TimerStart() {
+    std::pair<cudaEvent_t, cudaEvent_t> e;
+    cudaEventCreate(&e.first);
+    cudaEventCreate(&e.second);
+    cudaEventRecord(e.first, st_);
+    return e;
+  }
+  void TimerStop(std::pair<cudaEvent_t, cudaEvent_t> e) {
+    cudaEventRecord(e.second, st_);
+    events_.push_back(e);
+  }
+
+  void Scan(uint64_t* d, uint32_t n) {
+    if (n == 0) return;
+    uint32_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    size_t m = A_.Mark();
+    uint64_t* bs = (uint64_t*)A_.Alloc((size_t)nb * 8);
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, st_>>>(d, n, bs);
+    k_scan_partials<<<1, 1024, 0, st_>>>(bs, nb);
+    k_scan_apply<<<nb, SCAN_THREADS, 0, st_>>>(d, n, bs);
+    launches_ += 3;
+    A_.Release(m);
+  }
+
+  uint64_t ReadU64(const uint64_t* d) {
+    CK(cudaMemcpyAsync(ctx_.h_pinned, d, 8, cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    return ctx_.h_pinned[0];
+  }
+
+  struct Batch {
+    uint32_t b0, b1;
+    uint64_t e0, e1;  // inclusive estimate before b0 / at b1-1
+  };
+
+  std::vector<Batch> Split(const uint64_t* incl, uint32_t P, double pf, double cf, uint64_t budget) {
+    std::vector<Batch> out;
+    if (P == 0) return out;
+    budget = std::max<uint64_t>(budget, 1 << 20);
+    const uint32_t K = (uint32_t)std::min<size_t>(ctx_.pinned_words / 2, 4096);
+    size_t m = A_.Mark();
+    uint64_t* d = (uint64_t*)A_.Alloc((size_t)K * 16);
+    uint32_t start = 0;
+    uint64_t e_start = 0;
+    while (start < P) {
+      k_split<<<(K + 255) / 256, 256, 0, st_>>>(incl, P, start, pf, cf, (double)budget, K, d);
+      Launched();
+      CK(cudaMemcpyAsync(ctx_.h_pinned, d, (size_t)K * 16, cudaMemcpyDeviceToHost, st_));
+      CK(cudaStreamSynchronize(st_));
+      const uint64_t* h = ctx_.h_pinned;
+      for (uint32_t k = 0; k < K && start < P; ++k) {
+        uint32_t end = (uint32_t)std::min<uint64_t>(h[2 * k], P);
+        if (end <= start) continue;
+        uint64_t e_end = h[2 * k + 1];
+        out.push_back(Batch{start, end, e_start, e_end});
+        start = end;
+        e_start = e_end;
+      }
+    }
+    A_.Release(m);
+    return out;
+  }
+
+  static DFront Slice(const DFront& F, uint32_t b0, uint32_t b1) {
+    DFront G = F;
+    G.P = b1 - b0;
+    for (int v = 0; v < MAXV; ++v) {
+      if (F.inst[v]) G.inst[v] = F.inst[v] + b0;
+      if (F.cidx[v]) G.cidx[v] = F.cidx[v] + b0;
+      else G.ident_off[v] = F.ident_off[v] + b0;
+    }
+    return G;
+  }
+
+  void Emit(const DFront& F) {
+    uint8_t sl[MAXV] = {0, 0, 0, 0, 0, 0};
+    for (int v = 0; v < prog_.n; ++v) sl[v] = prog_.out_slot[v];
+    k_emit<<<Grid(F.P, 256), 256, 0, st_>>>(F, (uint8_t)prog_.n, nullptr, sl[0], sl[1], sl[2], sl[3],
+                                            sl[4], sl[5], out_, cap_, ctrl_ + 2);
+    Launched();
+  }
+
+  void Level(size_t k, const DFront& F) {
+    if (F.P == 0) return;
+    if (k == prog_.steps.size()) {
+      if (prog_.enumerate) Emit(F);
+      return;
+    }
+    const Step& s = prog_.steps[k];
+    const DStep ds = ToDStep(s);
+    unsigned long long* acc = ctrl_;
+    uint32_t* err = (uint32_t*)(ctrl_ + 3);
+    switch (s.kind) {
+      case S_COMPUTE_COUNT: {
+        paths_ += F.P;
+        auto t = TimerStart();
+        k_compute<1><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, g_.row_ptrs, g_.cols, nullptr, 0,
+                                                            nullptr, nullptr, nullptr, 0, acc, err);
+        TimerStop(t);
+        Launched();
+        return;
+      }
+      case S_COUNT: {
+        if (s.direct) {
+          uint8_t us[3] = {0, 0, 0};
+          for (size_t i = 0; i < s.unmat.size() && i < 3; ++i) us[i] = s.unmat[i];
+          k_count_direct<<<Grid(F.P, 256), 256, 0, st_>>>(F, (uint8_t)s.unmat.size(), us[0], us[1], us[2],
+                                                          prog_.query_type, acc);
+        } else if (s.unmat.size() == 1) {
+          k_count1<<<Grid(F.P, 256), 256, 0, st_>>>(F, s.unmat[0], acc);
+        } else {
+          k_count2<<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, s.unmat[0], s.unmat[1], s.pair_op, acc);
+        }
+        Launched();
+        return;
+      }
+      default:
+        break;
+    }
+    const size_t mark0 = A_.Mark();
+    uint64_t* est = (uint64_t*)A_.Alloc((size_t)F.P * 8);
+    double pf = 0, cf = 0;
+    if (s.kind == S_COMPUTE || s.kind == S_PATH_COUNT) {
+      k_est_compute<<<Grid(F.P, 256), 256, 0, st_>>>(F, ds, g_.row_ptrs, est);
+      pf = 12 + 16;
+      cf = s.kind == S_COMPUTE ? 4 : 0;
+    } else {  // MATERIALIZE, FILTER
+      k_est_set<<<Grid(F.P, 256), 256, 0, st_>>>(F, s.u, est);
+      if (s.kind == S_FILTER) {
+        pf = 12 + 16;
+        cf = 4;
+      } else {
+        pf = 16;
+        cf = 4.0 * (s.mat_after.size() + s.sets_after.size()) + 16;
+      }
+    }
+    Launched();
+    Scan(est, F.P);
+    uint64_t budget = Budget(k);
+    // keep child counts of a batch within 31-bit path indices
+    budget = std::min<uint64_t>(budget, (uint64_t)(std::max(cf, 1.0) * 2.0e9));
+    std::vector<Batch> batches = Split(est, F.P, pf, cf, budget);
+    for (const Batch& b : batches) {
+      const size_t mark = A_.Mark();
+      DFront Fb = Slice(F, b.b0, b.b1);
+      const uint32_t Pb = b.b1 - b.b0;
+      ++batches_;
+      switch (s.kind) {
+        case S_COMPUTE:
+        case S_PATH_COUNT: {
+          paths_ += Pb;
+          uint64_t* ptr = (uint64_t*)A_.Alloc((size_t)Pb * 8);
+          uint32_t* cnt = (uint32_t*)A_.Alloc((size_t)Pb * 4);
+          uint64_t cap = s.kind == S_COMPUTE ? b.e1 - b.e0 : 0;
+          uint32_t* data = cap ? (uint32_t*)A_.Alloc(cap * 4) : nullptr;
+          auto t = TimerStart();
+          if (s.kind == S_COMPUTE)
+            k_compute<0><<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, ds, g_.row_ptrs, g_.cols, est, b.b0, ptr,
+                                                               cnt, data, cap, acc, err);
+          else
+            k_compute<2><<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, ds, g_.row_ptrs, g_.cols, est, b.b0, ptr,
+                                                               cnt, nullptr, 0, acc, err);
+          TimerStop(t);
+          Launched();
+          DFront Fn = Fb;
+          Fn.set[s.u] = DSet{ptr, cnt};
+          Fn.cidx[s.u] = nullptr;
+          Fn.ident_off[s.u] = 0;
+          Level(k + 1, Fn);
+          break;
+        }
+        case S_FILTER: {
+          uint64_t* ptr = (uint64_t*)A_.Alloc((size_t)Pb * 8);
+          uint32_t* cnt = (uint32_t*)A_.Alloc((size_t)Pb * 4);
+          uint64_t cap = b.e1 - b.e0;
+          uint32_t* data = cap ? (uint32_t*)A_.Alloc(cap * 4) : nullptr;
+          k_filter<<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, s.u, ToDCond(s.cond), est, b.b0, ptr, cnt, data,
+                                                         cap, err);
+          Launched();
+          DFront Fn = Fb;
+          Fn.set[s.u] = DSet{ptr, cnt};
+          Fn.cidx[s.u] = nullptr;
+          Fn.ident_off[s.u] = 0;
+          Level(k + 1, Fn);
+          break;
+        }
+        case S_MATERIALIZE: {
+          DCond dc = ToDCond(s.cond);
+          uint64_t* cnt = (uint64_t*)A_.Alloc((size_t)Pb * 8);
+          k_mat_count<<<Grid(Pb, 256), 256, 0, st_>>>(Fb, s.u, dc, cnt);
+          Launched();
+          Scan(cnt, Pb);
+          uint64_t C = ReadU64(cnt + Pb - 1);
+          if (C == 0) break;
+          if (C > 0x7fffffffULL) Fail(SME_ERR_OOM, "materialised batch exceeds 2^31 partial instances");
+          DMatOut o{};
+          o.u = s.u;
+          o.keep = s.keep_set;
+          o.nmat = (uint8_t)s.mat_after.size();
+          for (size_t i = 0; i < s.mat_after.size(); ++i) {
+            o.mat[i] = s.mat_after[i];
+            o.inst[s.mat_after[i]] = (uint32_t*)A_.Alloc(C * 4);
+          }
+          o.nsets = (uint8_t)s.sets_after.size();
+          for (size_t i = 0; i < s.sets_after.size(); ++i) {
+            o.sets[i] = s.sets_after[i];
+            o.cidx[s.sets_after[i]] = (uint32_t*)A_.Alloc(C * 4);
+          }
+          auto t = TimerStart();
+          k_mat_write<<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, dc, o, cnt, C, err);
+          TimerStop(t);
+          Launched();
+          DFront Fn{};
+          Fn.P = (uint32_t)C;
+          for (int v = 0; v < MAXV; ++v) Fn.inst[v] = o.inst[v];
+          for (uint8_t w : s.sets_after) {
+            Fn.set[w] = Fb.set[w];
+            Fn.cidx[w] = o.cidx[w];
+          }
+          Level(k + 1, Fn);
+          break;
+        }
+        default:
+          Fail(SME_ERR_INVALID_ARG, "unexpected step kind");
+      }
+      A_.Release(mark);
+    }
+    A_.Release(mark0);
+  }
+};
+
+}  // namespace
+
+RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx, uint64_t rb,
+                     uint64_t re, uint32_t* d_out, uint64_t cap, int warp_granularity) {
+  (void)warp_granularity;
+  CK(cudaSetDevice(ctx.device));
+  if (re > g.n) re = g.n;
+  if (rb > re) rb = re;
+  Executor ex(prog, g, ctx, d_out, cap);
+  return ex.Run(rb, re);
+}
+
+}  // namespace sme

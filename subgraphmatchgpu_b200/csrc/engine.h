@@ -1,0 +1,67 @@
+// Device engine interface (engine.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sme_internal.h"
+
+namespace sme {
+
+// Resident device copy of a CSR graph.
+struct DeviceGraph {
+  int device = -1;
+  uint64_t n = 0, m = 0;
+  uintE* row_ptrs = nullptr;
+  uintV* cols = nullptr;
+  bool host_mapped = false;  // cols live in mapped pinned host memory (EXT_UMA)
+};
+
+// Stack allocator over one device allocation.  Levels are processed depth
+// first, so every allocation of a level batch is released (in LIFO order)
+// before the next batch of the same level starts.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, top = 0, peak = 0;
+  void* Alloc(size_t bytes);
+  size_t Mark() const { return top; }
+  void Release(size_t mark) { top = mark; }
+  size_t Free() const { return cap - top; }
+};
+
+// Per-device execution context: stream, arena, pinned staging buffers.
+struct DeviceContext {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Arena arena;
+  uint64_t* h_pinned = nullptr;  // small pinned host buffer for batch bounds
+  size_t pinned_words = 0;
+  ~DeviceContext();
+};
+
+// Allocates a context with an arena of `bytes` (0 = most of free memory).
+DeviceContext* CreateContext(int device, uint64_t bytes);
+void DestroyContext(DeviceContext* c);
+
+DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, uint64_t* h2d_bytes);
+void FreeDeviceGraph(DeviceGraph* d);
+
+struct RunResult {
+  uint64_t count = 0;
+  uint64_t emitted = 0;
+  sme_stats stats{};
+};
+
+// Runs `prog` over the root range [root_begin, root_end) of `g`.  When
+// prog.enumerate, instances are written to out (device) up to cap.
+RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx,
+                     uint64_t root_begin, uint64_t root_end, uint32_t* d_out, uint64_t cap,
+                     int warp_granularity);
+
+// External (chunked) execution over a graph that stays in host memory.
+RunResult RunProgramExternal(const Program& prog, const HostGraph& g, DeviceContext& ctx,
+                             uint64_t root_begin, uint64_t root_end, int ext_variant,
+                             uint64_t graph_budget_bytes);
+
+int DeviceCount();
+
+}  // namespace sme

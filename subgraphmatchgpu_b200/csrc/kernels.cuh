@@ -1,0 +1,165 @@
+// Device kernels of the enumeration engine (sm_100a, integer SIMT).
+//
+// A level frontier is a set of partial instances ("paths").  For each
+// pattern vertex it holds either a materialised column (one data vertex per
+// path) or a candidate set per path.  Candidate sets are (pointer, count)
+// pairs: the pointer is an absolute device address, so a set can be a
+// sub-range of an adjacency list or of a parent's set (zero copy) or live in
+// a level's own data buffer.
+#pragma once
+
+#include <cstdint>
+
+namespace sme {
+namespace dev {
+
+constexpr int MAXV = 6;  // kMaxQueryVerticesNum, src/Meta.h:30
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int WARP_BLOCK = 256;  // threads per block of warp-per-path kernels
+constexpr uint32_t ENGINE_ERR_BOUNDS = 1u;  // a write would leave its buffer
+
+struct DSet {
+  const uint64_t* ptr;  // absolute device address of the first element
+  const uint32_t* cnt;
+};
+
+struct DFront {
+  uint32_t P;                     // paths in this view
+  const uint32_t* inst[MAXV];     // materialised columns (null if none)
+  const uint32_t* cidx[MAXV];     // set index per path (null: identity)
+  uint32_t ident_off[MAXV];       // identity index offset (after slicing)
+  DSet set[MAXV];                 // candidate-set stores
+};
+
+struct DCond {
+  uint8_t n;
+  uint8_t op[MAXV];       // 0 <, 1 >, 2 !=
+  uint8_t operand[MAXV];  // materialised pattern vertex
+};
+
+struct DStep {
+  uint8_t u;
+  uint8_t nconn;
+  uint8_t conn[MAXV];
+  int8_t reuse;   // vertex whose candidate set joins the intersection
+  DCond cond;
+  int8_t with_u;  // COMPUTE_COUNT rank partner (-1 none)
+  uint8_t with_op;
+};
+
+struct DMatOut {
+  uint32_t* inst[MAXV];
+  uint32_t* cidx[MAXV];
+  uint8_t nmat, mat[MAXV];
+  uint8_t nsets, sets[MAXV];
+  uint8_t u;
+  uint8_t keep;
+};
+
+__device__ __forceinline__ uint32_t SetIndex(const DFront& F, int u, uint32_t p) {
+  const uint32_t* c = F.cidx[u];
+  return c ? c[p] : p + F.ident_off[u];
+}
+
+__device__ __forceinline__ void GetSet(const DFront& F, int u, uint32_t p, const uint32_t*& ptr,
+                                       uint32_t& len) {
+  uint32_t s = SetIndex(F, u, p);
+  ptr = reinterpret_cast<const uint32_t*>(F.set[u].ptr[s]);
+  len = F.set[u].cnt[s];
+}
+
+// First index i in a[0,n) with a[i] >= x (GpuUtils::BinSearch::BinSearch,
+// src/gpu/utils/ops/GPUBinSearch.cuh:18-31).
+__device__ __forceinline__ uint32_t LowerBound(const uint32_t* __restrict__ a, uint32_t n, uint32_t x) {
+  uint32_t lo = 0;
+  while (n > 0) {
+    uint32_t half = n >> 1;
+    if (__ldg(a + lo + half) < x) {
+      lo += half + 1;
+      n -= half + 1;
+    } else {
+      n = half;
+    }
+  }
+  return lo;
+}
+
+// Conditions of a candidate against materialised vertices reduce, on a sorted
+// list, to an interval [lo, hi) minus up to MAXV excluded values.
+struct Bounds {
+  uint64_t lo, hi;
+  uint32_t ne[MAXV];
+  int nne;
+};
+
+__device__ __forceinline__ Bounds MakeBounds(const DCond& c, const DFront& F, uint32_t p) {
+  Bounds b;
+  b.lo = 0;
+  b.hi = 1ULL << 32;
+  b.nne = 0;
+#pragma unroll
+  for (int i = 0; i < MAXV; ++i) {
+    if (i < c.n) {
+      uint32_t v = F.inst[c.operand[i]][p];
+      if (c.op[i] == 0) {
+        b.hi = min(b.hi, (uint64_t)v);
+      } else if (c.op[i] == 1) {
+        b.lo = max(b.lo, (uint64_t)v + 1);
+      } else {
+        b.ne[b.nne++] = v;
+      }
+    }
+  }
+  return b;
+}
+
+__device__ __forceinline__ void Range(const uint32_t* a, uint32_t n, const Bounds& b, uint32_t& r0,
+                                      uint32_t& r1) {
+  if (b.lo >= b.hi) {
+    r0 = r1 = 0;
+    return;
+  }
+  r0 = b.lo == 0 ? 0 : (b.lo > 0xffffffffULL ? n : LowerBound(a, n, (uint32_t)b.lo));
+  r1 = b.hi > 0xffffffffULL ? n : LowerBound(a, n, (uint32_t)b.hi);
+  if (r1 < r0) r1 = r0;
+}
+
+// Positions (ascending) of excluded values present in a[r0,r1).
+__device__ __forceinline__ int Exclusions(const uint32_t* a, uint32_t r0, uint32_t r1, const Bounds& b,
+                                          uint32_t* ex) {
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < MAXV; ++i) {
+    if (i < b.nne) {
+      uint32_t pos = r0 + LowerBound(a + r0, r1 - r0, b.ne[i]);
+      if (pos < r1 && __ldg(a + pos) == b.ne[i]) ex[k++] = pos;
+    }
+  }
+  for (int i = 1; i < k; ++i)  // insertion sort, k <= MAXV
+    for (int j = i; j > 0 && ex[j - 1] > ex[j]; --j) {
+      uint32_t t = ex[j];
+      ex[j] = ex[j - 1];
+      ex[j - 1] = t;
+    }
+  return k;
+}
+
+// Count of elements y of sorted s[0,n) with (x op y); op as CondOperator
+// (ThreadCountWithComputedVertex, src/gpu/impl/common/CheckConstraintsCommon.cuh:131-155).
+__device__ __forceinline__ uint64_t RankCount(const uint32_t* s, uint32_t n, uint32_t x, uint8_t op) {
+  if (n == 0) return 0;
+  uint32_t pos = LowerBound(s, n, x);
+  bool eq = pos < n && __ldg(s + pos) == x;
+  if (op == 0) return n - pos - (eq ? 1 : 0);  // x < y
+  if (op == 1) return pos;                     // x > y
+  return n - (eq ? 1 : 0);                     // x != y
+}
+
+__device__ __forceinline__ unsigned long long WarpSum(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+  return v;
+}
+
+}  // namespace dev
+}  // namespace sme

@@ -1,0 +1,66 @@
+"""ctypes loader of the CPU oracle (oracle/liboracle.so) -- test infrastructure.
+
+Used only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+the checker; the product never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+LIB = os.path.join(ROOT, "oracle", "liboracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+        L = C.CDLL(LIB)
+        L.oracle_wcoj.restype = C.c_uint64
+        L.oracle_wcoj.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_uint64, C.c_uint64,
+                                  C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]
+        L.oracle_query_size.restype = C.c_int
+        L.oracle_query_size.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def count(row_ptrs, cols, q, ordering=True, root_begin=0, root_end=0, threads=0) -> int:
+    rp = np.ascontiguousarray(row_ptrs, dtype=np.uint64)
+    cl = np.ascontiguousarray(cols, dtype=np.uint32)
+    return int(lib().oracle_wcoj(rp.ctypes.data, cl.ctypes.data if len(cl) else None, len(rp) - 1, q,
+                                 int(ordering), root_begin, root_end, threads, None, 0, None))
+
+
+def enumerate_sorted(row_ptrs, cols, q, ordering=True) -> np.ndarray:
+    rp = np.ascontiguousarray(row_ptrs, dtype=np.uint64)
+    cl = np.ascontiguousarray(cols, dtype=np.uint32)
+    k = lib().oracle_query_size(q)
+    n = count(rp, cl, q, ordering)
+    buf = np.zeros((max(n, 1), k), dtype=np.uint32)
+    got = C.c_uint64(0)
+    lib().oracle_wcoj(rp.ctypes.data, cl.ctypes.data if len(cl) else None, len(rp) - 1, q, int(ordering), 0, 0,
+                      0, buf.ctypes.data, n, C.byref(got))
+    out = buf[: got.value]
+    return sort_rows(out)
+
+
+def sort_rows(a: np.ndarray) -> np.ndarray:
+    if len(a) == 0:
+        return a
+    idx = np.lexsort(tuple(a[:, j] for j in reversed(range(a.shape[1]))))
+    return a[idx]
+
+
+def read_bin(path):
+    """BIN CSR reader for fixtures (4 x size_t header, row_ptrs, cols)."""
+    raw = open(path, "rb").read()
+    hdr = np.frombuffer(raw[:32], dtype=np.uint64)
+    n, m = int(hdr[2]), int(hdr[3])
+    rp = np.frombuffer(raw[32:32 + 8 * (n + 1)], dtype=np.uint64).copy()
+    cl = np.frombuffer(raw[32 + 8 * (n + 1):32 + 8 * (n + 1) + 4 * m], dtype=np.uint32).copy()
+    return rp, cl

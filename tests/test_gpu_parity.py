@@ -1,0 +1,157 @@
+"""GPU parity of the enumeration engine through the C-ABI (libsme.so).
+
+Counts are compared bit-exactly with the reference's own CPU program (golden
+counts) and with the C oracle; instance lists are compared sorted.
+"""
+import numpy as np
+import pytest
+
+import oracle_py as O
+import subgraphmatchgpu_b200 as sme
+from conftest import golden_graph_path
+
+pytestmark = pytest.mark.gpu
+
+ALGOS = (sme.GPU_GPSM, sme.GPU_GPSM_REUSE, sme.GPU_LIGHT)
+GPU_LIMIT = 3_000_000_000
+
+
+@pytest.fixture(scope="module")
+def graphs(golden):
+    return {name: sme.Graph.load(golden_graph_path(name)) for name in golden}
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_counts_match_reference_on_golden_graphs(graphs, golden, algo):
+    for name, d in golden.items():
+        g = graphs[name]
+        for q, want in d["counts"].items():
+            if want > GPU_LIMIT:
+                continue
+            got = g.count(int(q), algo, reuse_autogen=-1)
+            assert got == want, (name, q, algo, got, want)
+
+
+@pytest.mark.parametrize("level", [0, 1, 2, 3])
+def test_light_compress_levels(graphs, golden, level):
+    for name in ("rmat_s10_ef8", "ba_n600_m4", "k12"):
+        for q, want in golden[name]["counts"].items():
+            if want > GPU_LIMIT:
+                continue
+            assert graphs[name].count(int(q), sme.GPU_LIGHT, compress_level=level) == want, (name, q, level)
+
+
+def test_reuse_autogen_plans(graphs, golden):
+    for name in ("rmat_s10_ef8", "er_n64_d12"):
+        for q, want in golden[name]["counts"].items():
+            if want > GPU_LIMIT:
+                continue
+            assert graphs[name].count(int(q), sme.GPU_GPSM_REUSE, reuse_autogen=1) == want, (name, q)
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_sorted_instances_identical_to_oracle(graphs, algo):
+    for name in ("er_n64_d12", "k6", "ba_n600_m4"):
+        rp, cl = O.read_bin(golden_graph_path(name))
+        for q in (0, 1, 2, 3, 4, 7, 6, 9):
+            want = O.enumerate_sorted(rp, cl, q)
+            got = O.sort_rows(graphs[name].enumerate(q, algo))
+            assert got.shape == want.shape and np.array_equal(got, want), (name, q, algo)
+
+
+def test_ordering_disabled_counts_automorphic_images(graphs):
+    # -r 0: every automorphic image is counted (Query::DisableOrdering)
+    rp, cl = O.read_bin(golden_graph_path("er_n64_d12"))
+    for q in (0, 1, 3, 4):
+        want = O.count(rp, cl, q, ordering=False)
+        for algo in ALGOS:
+            assert graphs["er_n64_d12"].count(q, algo, enable_ordering=0) == want
+
+
+def test_root_ranges_sum_to_total(graphs, golden):
+    g = graphs["rmat_s12_ef8"]
+    n = g.n
+    for q in (0, 3, 1):
+        cuts = [0, 5, 100, n // 3, n]
+        parts = sum(g.count(q, sme.GPU_LIGHT, root_begin=a, root_end=b) for a, b in zip(cuts, cuts[1:]))
+        assert parts == golden["rmat_s12_ef8"]["counts"][str(q)]
+
+
+def test_small_memory_budget_forces_many_batches(graphs, golden):
+    g = graphs["rmat_s12_ef8"]
+    for algo in ALGOS:
+        for q in (3, 1, 4):
+            got = g.count(q, algo, mem_limit_bytes=24 << 20)
+            assert got == golden["rmat_s12_ef8"]["counts"][str(q)], (algo, q)
+            assert sme.last_stats().batches > 3
+
+
+def test_edge_cases():
+    # empty-ish, single edge, star, path, triangle
+    def csr(n, edges):
+        adj = [[] for _ in range(n)]
+        for u, v in edges:
+            adj[u].append(v)
+            adj[v].append(u)
+        rp = np.zeros(n + 1, np.uint64)
+        for u in range(n):
+            rp[u + 1] = rp[u] + len(adj[u])
+        cl = np.array([v for u in range(n) for v in sorted(adj[u])], np.uint32)
+        return rp, cl
+
+    cases = {
+        "single_edge": (2, [(0, 1)]),
+        "star": (9, [(0, i) for i in range(1, 9)]),
+        "path": (7, [(i, i + 1) for i in range(6)]),
+        "triangle": (3, [(0, 1), (1, 2), (0, 2)]),
+        "two_k4": (8, [(a, b) for a in range(4) for b in range(a + 1, 4)] +
+                   [(a, b) for a in range(4, 8) for b in range(a + 1, 8)]),
+    }
+    for name, (n, e) in cases.items():
+        rp, cl = csr(n, e)
+        g = sme.Graph.from_csr(rp, cl)
+        for q in (0, 1, 2, 3, 4, 7):
+            want = O.count(rp, cl, q)
+            for algo in ALGOS:
+                assert g.count(q, algo) == want, (name, q, algo)
+    g = sme.Graph.from_csr(np.zeros(1, np.uint64), np.zeros(0, np.uint32))
+    assert g.count(0) == 0
+
+
+def test_resident_graph_and_stats():
+    g = sme.Graph.rmat(14, 8, seed=1)
+    rp, cl = g.csr()
+    want = O.count(rp, cl, 0)
+    assert g.count(0) == want
+    s0 = sme.last_stats()
+    assert s0.h2d_bytes > 0
+    g.to_device(0)
+    assert g.count(0) == want
+    s = sme.last_stats()
+    assert s.h2d_bytes == 0 and s.kernel_launches > 0 and s.algorithmic_bytes > 0
+    for algo in ALGOS:
+        assert g.count(0, algo) == want
+
+
+def test_plans_agree_at_scale():
+    g = sme.Graph.rmat(16, 16, seed=3)
+    g.to_device(0)
+    for q in (0, 2, 3, 7):
+        c = [g.count(q, a) for a in ALGOS]
+        assert c[0] == c[1] == c[2], (q, c)
+
+
+def test_invalid_options_fail_cleanly():
+    g = sme.Graph.clique(5)
+    with pytest.raises(sme.SmeError) as e:
+        g.count(14)
+    assert e.value.status == 6
+    with pytest.raises(sme.SmeError):
+        g.count(0, algo=3)
+    with pytest.raises(sme.SmeError):
+        g.count(0, mode=0)
+    with pytest.raises(sme.SmeError) as e:
+        g.count(1, sme.GPU_GPSM_REUSE, reuse_autogen=0)
+    assert e.value.status == 6
+    # the context stays usable
+    assert g.count(0) == 10

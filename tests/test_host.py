@@ -1,0 +1,136 @@
+"""Host-side logic of libsme without a GPU: the C-ABI surface, formats,
+preprocessing, generators and the three query plans."""
+import hashlib
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+import subgraphmatchgpu_b200 as sme
+from conftest import ROOT, golden_graph_path
+
+HEADER = os.path.join(ROOT, "include", "sme.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sme_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = sme.lib()
+    names = header_functions()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in sme.SIGNATURES, f"{n} missing from the Python signature table"
+
+
+def test_version_and_opts_defaults():
+    assert b"sm_100a" in sme.lib().sme_version()
+    o = sme.opts(3)
+    assert (o.algo, o.execute_mode, o.compress_level, o.enable_ordering) == (6, 1, 3, 1)
+
+
+def sha(path):
+    return hashlib.sha256(open(path, "rb").read()).hexdigest()
+
+
+def test_bin_roundtrip_is_byte_identical(tmp_path, golden):
+    for name in ("k6", "rmat_s10_ef8", "ba_n600_m4"):
+        g = sme.Graph.load(golden_graph_path(name))
+        out = str(tmp_path / "x.bin")
+        g.write_bin(out)
+        assert sha(out) == golden[name]["sha256"]
+        g.validate()
+
+
+def test_generators_are_deterministic(golden):
+    g = sme.Graph.rmat(10, 8, seed=12)
+    n, m, d = g.info()
+    assert (n, m, d) == (golden["rmat_s10_ef8"]["n"], golden["rmat_s10_ef8"]["m"], golden["rmat_s10_ef8"]["max_degree"])
+    g.validate()
+    g2 = sme.Graph.rmat(10, 8, seed=12)
+    for a, b in zip(g.csr(), g2.csr()):
+        assert np.array_equal(a, b)
+    for h in (sme.Graph.er(300, 6.0, seed=3), sme.Graph.ba(300, 3, seed=3), sme.Graph.clique(7)):
+        h.validate()
+
+
+def test_preprocess_matches_reference_preprocess_graph(tmp_path):
+    rec = json.load(open(os.path.join(ROOT, "tests", "golden", "preprocess.json")))
+    g = sme.Graph.load(os.path.join(ROOT, "tests", "golden", "messy_edges.txt"), 0)
+    g.preprocess()
+    out = str(tmp_path / "m.bin")
+    g.write_bin(out)
+    assert sha(out) == rec["reference_sha256"] == rec["libsme_sha256"]
+
+
+def test_bad_inputs_return_status(tmp_path):
+    p = tmp_path / "trunc.bin"
+    p.write_bytes(b"\x04" + b"\x00" * 20)
+    with pytest.raises(sme.SmeError) as e:
+        sme.Graph.load(str(p))
+    assert e.value.status == 2
+    src = open(golden_graph_path("k6"), "rb").read()
+    p.write_bytes(src[:-3])
+    with pytest.raises(sme.SmeError):
+        sme.Graph.load(str(p))
+    p.write_bytes(src[:8] + (5).to_bytes(8, "little") + src[16:])  # uintE size 5
+    with pytest.raises(sme.SmeError):
+        sme.Graph.load(str(p))
+    with pytest.raises(sme.SmeError):
+        sme.Graph.load(str(tmp_path / "missing.bin"))
+    with pytest.raises(sme.SmeError) as e:
+        sme.plan_describe(14, 2)
+    assert e.value.status == 6
+    with pytest.raises(sme.SmeError):
+        sme.Graph.from_csr(np.array([0, 2, 1], np.uint64), np.array([1, 0], np.uint32))
+    with pytest.raises(sme.SmeError):
+        sme.Graph.from_csr(np.array([0, 1, 2], np.uint64), np.array([1, 5], np.uint32))
+
+
+@pytest.mark.parametrize("q", range(14))
+def test_light_plan_matches_reference_test_plan(q):
+    ref = open(os.path.join(ROOT, "tests", "golden", "plans", f"q{q}_light_nonmat_opt.txt")).read()
+    block = ref.split(f"Lazy traversal plan for Q{q}--------------------\n")[1].split("-----")[0]
+    mine = sme.plan_describe(q, 2).strip().splitlines()[1:]
+    assert block.strip().splitlines() == mine
+
+
+@pytest.mark.parametrize("q", range(14))
+def test_reuse_autogen_plan_matches_reference_test_plan(q):
+    ref = open(os.path.join(ROOT, "tests", "golden", "plans", f"q{q}_reuse_autogen.txt")).read()
+    rl = [l for l in ref.splitlines() if l.startswith("level ")]
+    ml = [l.split("  (cached)")[0] for l in sme.plan_describe(q, 1).splitlines() if l.startswith("level ")]
+    assert rl == ml
+
+
+def test_special_plans_and_hardcoded_reuse():
+    # COMPRESS_LEVEL_SPECIAL (LazyTraversalPlanGenerator.h:244-300)
+    q2 = sme.plan_describe(2, 4)
+    assert "(COMPUTE_PATH_COUNT,1),(COMPUTE_PATH_COUNT,3),(COUNT,4)" in q2
+    assert "(COUNT,6)" in sme.plan_describe(5, 4)
+    # hard-coded reuse plans exist for Q0,Q2,Q3,Q7,Q11; Q1/Q4 have none
+    for q in (0, 2, 3, 7, 11):
+        sme.plan_describe(q, 3)
+    for q in (1, 4):
+        with pytest.raises(sme.SmeError) as e:
+            sme.plan_describe(q, 3)
+        assert e.value.status == 6
+    q7 = sme.plan_describe(7, 3)
+    assert "level 4, vertex=4:intersect: [source_vertex=3,conn=(0,1,2),source_conn=(0,1,2)] 3" in q7
+
+
+def test_compiled_programs_are_consistent():
+    for q in range(14):
+        text = sme.plan_describe(q, 5)
+        assert text.count("program Q") == 3
+        # every program starts with the roots and ends in a counting step
+        for prog in text.split("program Q")[1:]:
+            lines = prog.strip().splitlines()[1:]
+            assert lines[0].split(":")[1].strip().startswith("INIT")
+            assert re.search(r"(COMPUTE_COUNT|COUNT)\(", lines[-1])
