@@ -93,6 +93,9 @@ typedef struct sme_stats {
   uint64_t d2h_bytes;
   uint64_t peak_device_bytes; /* high-water mark of the frontier arena       */
   uint64_t paths_processed;   /* partial instances entering compute steps    */
+  double device_ms;           /* CUDA-event time on the library's stream from
+                                 the first to the last kernel of the run      */
+  uint64_t hot_launches;      /* launches of the intersection kernels         */
 } sme_stats;
 
 /* ---- options ------------------------------------------------------------- */

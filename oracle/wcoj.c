@@ -301,3 +301,36 @@ uint64_t oracle_wcoj(const uint64_t* rp, const uint32_t* cols, uint64_t nv, int 
   if (n_written) *n_written = pos;
   return total;
 }
+
+/*
+ * Strided root sample: counts instances rooted at r = offset + k*stride for
+ * all k with r < nv (the bounded CPU-baseline sample of a large graph).
+ */
+uint64_t oracle_wcoj_strided(const uint64_t* rp, const uint32_t* cols, uint64_t nv, int q, int ordering,
+                             uint64_t stride, uint64_t offset, int threads) {
+  pattern_t p;
+  if (build_pattern(q, &p) || stride == 0) return (uint64_t)-1;
+  plan_t pl;
+  make_plan(&p, ordering, &pl);
+  uint64_t pos = 0;
+  ctx_t c = {rp, cols, nv, &pl, NULL, 0, &pos};
+  uint64_t maxd = max_degree(rp, nv);
+  size_t per_thread = (size_t)(3 * maxd + 3) * (size_t)(MAXQ + 1);
+  uint64_t total = 0;
+  long long cnt = offset < nv ? (long long)((nv - offset + stride - 1) / stride) : 0;
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel reduction(+ : total)
+  {
+    uint32_t* buf = (uint32_t*)malloc(sizeof(uint32_t) * per_thread);
+    uint32_t path[MAXQ];
+#pragma omp for schedule(dynamic, 1)
+    for (long long k = 0; k < cnt; ++k) {
+      path[0] = (uint32_t)(offset + (uint64_t)k * stride);
+      total += dfs(&c, 1, path, buf);
+    }
+    free(buf);
+  }
+  return total;
+}

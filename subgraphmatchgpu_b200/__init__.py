@@ -59,6 +59,7 @@ class Stats(C.Structure):
         ("elapsed_ms", C.c_double), ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64),
         ("batches", C.c_uint64), ("algorithmic_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64),
         ("d2h_bytes", C.c_uint64), ("peak_device_bytes", C.c_uint64), ("paths_processed", C.c_uint64),
+        ("device_ms", C.c_double), ("hot_launches", C.c_uint64),
     ]
 
 
@@ -289,7 +290,106 @@ class Graph:
             pass
 
 
+class BatchPlan:
+    """Batched form: many small (graph, query) pairs, one persistent launch
+    captured in a CUDA graph, group size and block shape autotuned."""
+
+    def __init__(self, graphs: Sequence[Graph], queries: Sequence[int], autotune: bool = True,
+                 use_graph: bool = True, device: int = 0, granularity: int = 0, block_threads: int = 0):
+        o = BatchOpts()
+        _check(lib().sme_batch_opts_default(C.byref(o)))
+        o.autotune, o.use_graph, o.device = int(autotune), int(use_graph), device
+        o.granularity, o.block_threads = granularity, block_threads
+        self._graphs = list(graphs)
+        hs = (C.c_void_p * len(graphs))(*[g.handle.value for g in graphs])
+        qs = np.ascontiguousarray(queries, dtype=np.int32)
+        self._h = C.c_void_p()
+        _check(lib().sme_batch_prepare(hs, qs.ctypes.data, len(graphs), C.byref(o), C.byref(self._h)))
+        self.num = len(graphs)
+
+    def run(self):
+        counts = np.zeros(self.num, dtype=np.uint64)
+        ms = C.c_double(0)
+        _check(lib().sme_batch_run(self._h, counts.ctypes.data, C.byref(ms)))
+        return counts, ms.value
+
+    def describe(self):
+        g, b, n = C.c_int32(), C.c_int32(), C.c_uint64()
+        _check(lib().sme_batch_describe(self._h, C.byref(g), C.byref(b), C.byref(n)))
+        return {"group_threads": g.value, "block_threads": b.value, "work_items": n.value}
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().sme_batch_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Served form: resident graphs, admission by estimated frontier memory,
+    concurrent requests across slots (continuous batching)."""
+
+    def __init__(self, slots: int = 4, mem_budget_bytes: int = 0, device: int = 0, queue_capacity: int = 1 << 16):
+        o = ServerOpts()
+        _check(lib().sme_server_opts_default(C.byref(o)))
+        o.slots, o.mem_budget_bytes, o.device, o.queue_capacity = slots, mem_budget_bytes, device, queue_capacity
+        self._h = C.c_void_p()
+        _check(lib().sme_server_create(C.byref(o), C.byref(self._h)))
+        self._keep = []
+
+    def add_graph(self, g: Graph) -> int:
+        gid = C.c_int32()
+        _check(lib().sme_server_add_graph(self._h, g.handle, C.byref(gid)))
+        self._keep.append(g)
+        return gid.value
+
+    def submit(self, query: int, gid: int = -1, attached: Optional[Graph] = None, algo: int = GPU_LIGHT,
+               **kw) -> int:
+        o = opts(query, algo, IN_MEMORY_GPU, **kw)
+        rid = C.c_uint64()
+        if attached is not None:
+            self._keep.append(attached)
+        _check(lib().sme_server_submit(self._h, gid, attached.handle if attached is not None else None,
+                                       C.byref(o), C.byref(rid)))
+        return rid.value
+
+    def poll(self, rid: int):
+        c, lat = C.c_uint64(), C.c_double()
+        st = lib().sme_server_poll(self._h, rid, C.byref(c), C.byref(lat))
+        if st == 9:
+            return None
+        _check(st)
+        return c.value, lat.value
+
+    def wait(self, rid: int):
+        c, lat = C.c_uint64(), C.c_double()
+        _check(lib().sme_server_wait(self._h, rid, C.byref(c), C.byref(lat)))
+        return c.value, lat.value
+
+    def stats(self):
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(lib().sme_server_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"completed": a.value, "max_inflight": b.value, "rejected": c.value}
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().sme_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 __all__ = [
+    "BatchPlan", "Server",
     "Graph", "SmeError", "Opts", "Stats", "lib", "opts", "plan_describe", "last_stats", "query_vertex_count",
     "GPU_GPSM", "GPU_GPSM_REUSE", "GPU_LIGHT", "IN_MEMORY_GPU", "EXTERNAL_GPU", "SIGNATURES", "QUERY_NAMES",
 ]

@@ -1,7 +1,562 @@
-// Batched form: placeholder.
+// Batched form: thousands of small (graph, query) pairs in one persistent
+// launch, captured in a CUDA graph.
+//
+// Every graph is packed into one CSR (local vertex ids); the work items are
+// (graph, root vertex) pairs ordered heaviest first.  A persistent grid of
+// thread groups (4..32 lanes) pulls items from an atomic counter and runs a
+// depth-first enumeration of the item's root: each level's candidate set is
+// computed cooperatively by the group (pivot list clipped by the order
+// constraints, binary search in the other lists, ballot compaction), kept as a
+// view of an adjacency list when it is one, else in the group's scratch
+// buffer; the last level is only counted.  Counts accumulate per graph.
+//
+// An autotuner times every (group size, block size) candidate on the batch
+// itself and keeps the fastest; the winner is captured in a CUDA graph that
+// sme_batch_run replays.  Per-level semantics follow the plain traversal plan
+// (ordered backward connectivity + whole-ordered conditions,
+// src/gpu/plan/DevTraversalPlan.cuh:9-16); cliques reuse the previous level's
+// set (their chain order implies every earlier condition) and the diamond
+// uses the closed form of LIGHTDirectCount (c(c-1)/2 per edge,
+// src/gpu/impl/light/op/LIGHTDirectCount.cuh:31-37).
+#include <algorithm>
+#include <chrono>
+#include <memory>
+#include <vector>
+
 #include "engine.h"
+#include "kernels.cuh"
+
+namespace sme {
+using namespace dev;
+
+#define BCK(x)                                                                                 \
+  do {                                                                                         \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess) Fail(SME_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+
+constexpr int BMAXV = 6;
+
+struct BLevel {
+  uint8_t nconn;
+  uint8_t conn[BMAXV];
+  int8_t reuse;  // earlier level whose set joins the intersection
+  uint8_t ncond;
+  uint8_t op[BMAXV];
+  uint8_t operand[BMAXV];
+};
+struct BProg {
+  uint8_t n;         // pattern vertices; levels 1..n-1
+  uint8_t pair;      // last level adds c*(c-1)/2 instead of c
+  uint8_t buffered[BMAXV];  // level needs a scratch buffer (multi-list)
+  uint8_t buf_slot[BMAXV];
+  BLevel lv[BMAXV];
+};
+
+__constant__ BProg c_prog[SME_NUM_QUERIES];
+
+struct BArgs {
+  const uint32_t* rp;    // packed row pointers (uint32 offsets into cols)
+  const uint32_t* cols;  // packed local ids
+  const uint32_t* goff;  // graph -> first row pointer index
+  const uint8_t* query;  // graph -> query id
+  const uint64_t* items; // (graph << 32) | root
+  uint64_t nitems;
+  unsigned long long* counts;
+  unsigned int* next;
+  uint32_t* scratch;     // per group: nbuf * cap uint32
+  uint32_t cap;          // max degree in the batch
+  uint32_t nbuf;
+};
+
+template <int G>
+struct Tile {
+  int lane;            // lane within the group
+  unsigned mask;       // lanes of this group within the warp
+  int base;            // first lane of the group in the warp
+  __device__ Tile() {
+    int l = threadIdx.x & 31;
+    lane = l % G;
+    base = l - lane;
+    mask = (G == 32) ? FULL : (((1u << G) - 1) << base);
+  }
+  __device__ unsigned ballot(bool b) const { return (__ballot_sync(mask, b) & mask) >> base; }
+  __device__ uint32_t bcast(uint32_t v) const { return __shfl_sync(mask, v, base); }
+  __device__ unsigned long long sum(unsigned long long v) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_down_sync(mask, v, o, G);
+    return v;
+  }
+};
+
+// Candidate set of level `l` for the current partial instance M: written to
+// `out` (when non-null) or counted.  Returns the group-uniform size; when the
+// set is a single clipped list without exclusions, *view points into it.
+template <int G>
+__device__ uint32_t LevelSet(const Tile<G>& t, const BLevel& L, const uint32_t* M, const uint32_t* rp,
+                             const uint32_t* cols, const uint32_t* const* sptr, const uint32_t* slen,
+                             uint32_t* out, const uint32_t** view, bool pair_count,
+                             unsigned long long* cnt) {
+  const uint32_t* A[BMAXV];
+  uint32_t N[BMAXV];
+  int nl = 0;
+#pragma unroll
+  for (int i = 0; i < BMAXV; ++i) {
+    if (i < L.nconn) {
+      uint32_t v = M[L.conn[i]];
+      A[i] = cols + rp[v];
+      N[i] = rp[v + 1] - rp[v];
+      nl = i + 1;
+    }
+  }
+  if (L.reuse >= 0) {
+#pragma unroll
+    for (int i = 0; i < BMAXV; ++i)
+      if (i == nl) {
+        A[i] = sptr[L.reuse];
+        N[i] = slen[L.reuse];
+      }
+    ++nl;
+  }
+#pragma unroll
+  for (int i = 1; i < BMAXV; ++i) {
+    if (i < nl && N[i] < N[0]) {
+      const uint32_t* tp = A[0];
+      A[0] = A[i];
+      A[i] = tp;
+      uint32_t tn = N[0];
+      N[0] = N[i];
+      N[i] = tn;
+    }
+  }
+  uint64_t lo = 0, hi = 1ULL << 32;
+  uint32_t ne[BMAXV];
+  int nne = 0;
+#pragma unroll
+  for (int i = 0; i < BMAXV; ++i) {
+    if (i < L.ncond) {
+      uint32_t v = M[L.operand[i]];
+      if (L.op[i] == 0) hi = min(hi, (uint64_t)v);
+      else if (L.op[i] == 1) lo = max(lo, (uint64_t)v + 1);
+      else ne[nne++] = v;
+    }
+  }
+  if (lo >= hi || nl == 0) return 0;
+  uint32_t r0 = lo == 0 ? 0 : (lo > 0xffffffffULL ? N[0] : LowerBound(A[0], N[0], (uint32_t)lo));
+  uint32_t r1 = hi > 0xffffffffULL ? N[0] : LowerBound(A[0], N[0], (uint32_t)hi);
+  if (r1 < r0) r1 = r0;
+  if (nl == 1 && view) {
+    bool hit = false;
+    for (int k = 0; k < nne; ++k) {
+      uint32_t pos = r0 + LowerBound(A[0] + r0, r1 - r0, ne[k]);
+      if (pos < r1 && A[0][pos] == ne[k]) hit = true;
+    }
+    if (!hit) {
+      *view = A[0] + r0;
+      if (cnt) {
+        unsigned long long c = r1 - r0;
+        *cnt += pair_count ? (c > 0 ? c * (c - 1) / 2 : 0) : c;
+      }
+      return r1 - r0;
+    }
+  }
+  uint32_t cur[BMAXV];
+#pragma unroll
+  for (int i = 0; i < BMAXV; ++i) cur[i] = 0;
+  uint32_t written = 0;
+  for (uint32_t b = r0; b < r1; b += G) {
+    uint32_t i = b + t.lane;
+    bool ok = i < r1;
+    uint32_t x = ok ? __ldg(A[0] + i) : 0;
+    for (int k = 0; k < nne; ++k)
+      if (x == ne[k]) ok = false;
+#pragma unroll
+    for (int j = 1; j < BMAXV; ++j) {
+      if (j < nl && ok) {
+        uint32_t pos = cur[j] + LowerBound(A[j] + cur[j], N[j] - cur[j], x);
+        cur[j] = pos;
+        ok = pos < N[j] && __ldg(A[j] + pos) == x;
+      }
+    }
+    unsigned m = t.ballot(ok);
+    if (out && ok) out[written + __popc(m & ((1u << t.lane) - 1))] = x;
+    written += __popc(m);
+  }
+  if (cnt) {
+    unsigned long long c = written;
+    *cnt += pair_count ? (c > 0 ? c * (c - 1) / 2 : 0) : c;
+  }
+  if (view) *view = out;
+  return written;
+}
+
+template <int G>
+__global__ void k_batch(BArgs a) {
+  Tile<G> t;
+  const uint32_t groups_per_block = blockDim.x / G;
+  const uint32_t gid = blockIdx.x * groups_per_block + threadIdx.x / G;
+  uint32_t* scratch = a.scratch + (size_t)gid * a.nbuf * a.cap;
+  while (true) {
+    uint32_t it = 0;
+    if (t.lane == 0) it = atomicAdd(a.next, 1u);
+    it = t.bcast(it);
+    if (it >= a.nitems) break;
+    const uint64_t item = a.items[it];
+    const uint32_t g = (uint32_t)(item >> 32);
+    const uint32_t root = (uint32_t)item;
+    const BProg& P = c_prog[a.query[g]];
+    const uint32_t* rp = a.rp + a.goff[g];
+    uint32_t M[BMAXV];
+    const uint32_t* sptr[BMAXV];
+    uint32_t slen[BMAXV], idx[BMAXV];
+    M[0] = root;
+    unsigned long long local = 0;
+    const int last = P.n - 1;
+    // level 1
+    int level = 1;
+    if (level == last) {
+      LevelSet<G>(t, P.lv[1], M, rp, a.cols, sptr, slen, nullptr, nullptr, P.pair, &local);
+    } else {
+      uint32_t* out = P.buffered[1] ? scratch + P.buf_slot[1] * a.cap : nullptr;
+      slen[1] = LevelSet<G>(t, P.lv[1], M, rp, a.cols, sptr, slen, out, &sptr[1], false, nullptr);
+      idx[1] = 0;
+      while (level >= 1) {
+        if (idx[level] < slen[level]) {
+          M[level] = sptr[level][idx[level]];
+          ++idx[level];
+          const int nx = level + 1;
+          if (nx == last) {
+            LevelSet<G>(t, P.lv[nx], M, rp, a.cols, sptr, slen, nullptr, nullptr, P.pair, &local);
+          } else {
+            uint32_t* out = P.buffered[nx] ? scratch + P.buf_slot[nx] * a.cap : nullptr;
+            slen[nx] = LevelSet<G>(t, P.lv[nx], M, rp, a.cols, sptr, slen, out, &sptr[nx], false, nullptr);
+            idx[nx] = 0;
+            level = nx;
+          }
+        } else {
+          --level;
+        }
+      }
+    }
+    // set sizes are group-uniform (ballot popcounts), so every lane holds the
+    // same count; the leader adds it
+    if (t.lane == 0 && local) atomicAdd(a.counts + g, local);
+  }
+}
+
+BProg CompileBatchProgram(int q) {
+  BProg p{};
+  Query query(q);
+  TraversalPlan tp(query);
+  p.n = (uint8_t)query.n;
+  if (q == 2) {
+    // diamond: edges (u0 < u2), c = |N(u0) ∩ N(u2)|, count c(c-1)/2
+    p.n = 3;
+    p.pair = 1;
+    p.lv[1].nconn = 1;
+    p.lv[1].conn[0] = 0;
+    p.lv[1].reuse = -1;
+    p.lv[1].ncond = 1;
+    p.lv[1].op[0] = LARGER_THAN;
+    p.lv[1].operand[0] = 0;
+    p.lv[2].nconn = 2;
+    p.lv[2].conn[0] = 0;
+    p.lv[2].conn[1] = 1;
+    p.lv[2].reuse = -1;
+    p.lv[2].ncond = 0;
+  } else {
+    const bool clique = q == 3 || q == 7 || q == 11 || q == 0;
+    for (int u = 1; u < query.n; ++u) {
+      BLevel& L = p.lv[u];
+      L.reuse = -1;
+      if (clique && u >= 2) {
+        // chain order u0 < u1 < ... : previous level's set ∩ N(M[u-1]) ∩ (> M[u-1])
+        L.nconn = 1;
+        L.conn[0] = (uint8_t)(u - 1);
+        L.reuse = (int8_t)(u - 1);
+        L.ncond = 1;
+        L.op[0] = LARGER_THAN;
+        L.operand[0] = (uint8_t)(u - 1);
+      } else {
+        L.nconn = (uint8_t)tp.ordered_conn[u].size();
+        for (size_t i = 0; i < tp.ordered_conn[u].size(); ++i) L.conn[i] = (uint8_t)tp.ordered_conn[u][i];
+        L.ncond = (uint8_t)tp.whole_order[u].size();
+        for (size_t i = 0; i < tp.whole_order[u].size(); ++i) {
+          L.op[i] = (uint8_t)tp.whole_order[u][i].first;
+          L.operand[i] = (uint8_t)tp.whole_order[u][i].second;
+        }
+      }
+    }
+  }
+  int slot = 0;
+  for (int u = 1; u + 1 < p.n; ++u) {
+    // a set needs storage unless it is always a clipped single list (a view):
+    // several lists, or an excluded value that may fall inside the range
+    int lists = p.lv[u].nconn + (p.lv[u].reuse >= 0 ? 1 : 0);
+    bool ne = false;
+    for (int i = 0; i < p.lv[u].ncond; ++i) ne = ne || p.lv[u].op[i] == NON_EQUAL;
+    if (lists > 1 || ne) {
+      p.buffered[u] = 1;
+      p.buf_slot[u] = (uint8_t)slot++;
+    }
+  }
+  return p;
+}
+
+void UploadPrograms(int device) {
+  static bool done[64] = {false};
+  if (device >= 0 && device < 64 && done[device]) return;
+  BProg all[SME_NUM_QUERIES];
+  for (int q = 0; q < SME_NUM_QUERIES; ++q) all[q] = CompileBatchProgram(q);
+  BCK(cudaMemcpyToSymbol(c_prog, all, sizeof(all)));
+  if (device >= 0 && device < 64) done[device] = true;
+}
+
+int MaxBuffers(const std::vector<int32_t>& queries) {
+  int nb = 0;
+  for (int q : queries) {
+    BProg p = CompileBatchProgram(q);
+    int c = 0;
+    for (int u = 0; u < BMAXV; ++u) c += p.buffered[u];
+    nb = std::max(nb, c);
+  }
+  return std::max(nb, 1);
+}
+
+}  // namespace
+}  // namespace sme
+
+using namespace sme;
+
+struct sme_batch_plan {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t num = 0, nitems = 0;
+  uint32_t cap = 1, nbuf = 1;
+  uint32_t *d_rp = nullptr, *d_cols = nullptr, *d_goff = nullptr, *d_scratch = nullptr;
+  uint8_t* d_query = nullptr;
+  uint64_t* d_items = nullptr;
+  unsigned long long* d_counts = nullptr;
+  unsigned int* d_next = nullptr;
+  int G = 8, block = 256, grid = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool use_graph = true;
+  ~sme_batch_plan() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void* p : {(void*)d_rp, (void*)d_cols, (void*)d_goff, (void*)d_scratch, (void*)d_query, (void*)d_items,
+                    (void*)d_counts, (void*)d_next})
+      if (p) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+BArgs Args(sme_batch_plan* p) {
+  BArgs a;
+  a.rp = p->d_rp;
+  a.cols = p->d_cols;
+  a.goff = p->d_goff;
+  a.query = p->d_query;
+  a.items = p->d_items;
+  a.nitems = p->nitems;
+  a.counts = p->d_counts;
+  a.next = p->d_next;
+  a.scratch = p->d_scratch;
+  a.cap = p->cap;
+  a.nbuf = p->nbuf;
+  return a;
+}
+
+int SmCountB(int device) {
+  int v = 148;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+  return v;
+}
+
+// Launches the persistent kernel with group size G and `block` threads on a
+// grid of resident blocks; the scratch holds a buffer set per group.
+void Launch(sme_batch_plan* p, int G, int block, int grid) {
+  BArgs a = Args(p);
+  switch (G) {
+    case 4: k_batch<4><<<grid, block, 0, p->stream>>>(a); break;
+    case 8: k_batch<8><<<grid, block, 0, p->stream>>>(a); break;
+    case 16: k_batch<16><<<grid, block, 0, p->stream>>>(a); break;
+    default: k_batch<32><<<grid, block, 0, p->stream>>>(a); break;
+  }
+}
+
+int GridFor(sme_batch_plan* p, int G, int block) {
+  int blocks_per_sm = 0;
+  switch (G) {
+    case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<4>, block, 0); break;
+    case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<8>, block, 0); break;
+    case 16: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<16>, block, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<32>, block, 0); break;
+  }
+  return std::max(1, blocks_per_sm) * SmCountB(p->device);
+}
+
+void Reset(sme_batch_plan* p) {
+  BCK(cudaMemsetAsync(p->d_counts, 0, p->num * sizeof(unsigned long long), p->stream));
+  BCK(cudaMemsetAsync(p->d_next, 0, sizeof(unsigned int), p->stream));
+}
+
+float TimeConfig(sme_batch_plan* p, int G, int block) {
+  int grid = GridFor(p, G, block);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  Reset(p);
+  Launch(p, G, block, grid);  // warm
+  Reset(p);
+  cudaEventRecord(e0, p->stream);
+  Launch(p, G, block, grid);
+  cudaEventRecord(e1, p->stream);
+  BCK(cudaStreamSynchronize(p->stream));
+  BCK(cudaGetLastError());
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+void Prepare(sme_graph* const* graphs, const int32_t* queries, uint64_t num, const sme_batch_opts& o,
+             sme_batch_plan* p) {
+  if (num == 0) Fail(SME_ERR_INVALID_ARG, "empty batch");
+  if (DeviceCount() <= o.device) Fail(SME_ERR_NO_DEVICE, "no CUDA device " + std::to_string(o.device));
+  BCK(cudaSetDevice(o.device));
+  p->device = o.device;
+  p->num = num;
+  p->use_graph = o.use_graph != 0;
+  BCK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  UploadPrograms(o.device);
+  std::vector<int32_t> qs(queries, queries + num);
+  for (int32_t q : qs)
+    if (q < 0 || q >= SME_NUM_QUERIES) Fail(SME_ERR_UNSUPPORTED_QUERY, "query out of range in batch");
+  // pack CSRs (uint32 offsets; graphs are small)
+  std::vector<uint32_t> rp, cols, goff(num);
+  std::vector<uint8_t> qv(num);
+  std::vector<std::pair<uint64_t, uint64_t>> work;  // (cost, item)
+  uint64_t maxdeg = 1;
+  for (uint64_t i = 0; i < num; ++i) {
+    const HostGraph& g = graphs[i]->g;
+    if (g.n >= (1ULL << 31)) Fail(SME_ERR_INVALID_ARG, "batched graphs must be small");
+    goff[i] = (uint32_t)rp.size();
+    qv[i] = (uint8_t)qs[i];
+    uint64_t base = cols.size();
+    if (base + g.m >= (1ULL << 32)) Fail(SME_ERR_INVALID_ARG, "batch too large for 32-bit packing");
+    for (uint64_t u = 0; u <= g.n; ++u) rp.push_back((uint32_t)(base + g.row_ptrs[u]));
+    cols.insert(cols.end(), g.cols, g.cols + g.m);
+    for (uint64_t u = 0; u < g.n; ++u) {
+      uint64_t d = g.row_ptrs[u + 1] - g.row_ptrs[u];
+      maxdeg = std::max(maxdeg, d);
+      // cost estimate: sum of neighbour degrees (two-level fan-out)
+      uint64_t c = 1;
+      for (uint64_t j = g.row_ptrs[u]; j < g.row_ptrs[u + 1]; ++j) {
+        uintV v = g.cols[j];
+        c += g.row_ptrs[v + 1] - g.row_ptrs[v];
+      }
+      work.emplace_back(c, (i << 32) | u);
+    }
+  }
+  std::stable_sort(work.begin(), work.end(), [](const std::pair<uint64_t, uint64_t>& a,
+                                                const std::pair<uint64_t, uint64_t>& b) { return a.first > b.first; });
+  std::vector<uint64_t> items(work.size());
+  for (size_t i = 0; i < work.size(); ++i) items[i] = work[i].second;
+  p->nitems = items.size();
+  p->cap = (uint32_t)maxdeg;
+  p->nbuf = (uint32_t)MaxBuffers(qs);
+  auto up = [&](void** dst, const void* src, size_t bytes) {
+    BCK(cudaMalloc(dst, std::max<size_t>(bytes, 4)));
+    if (bytes) BCK(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, p->stream));
+  };
+  up((void**)&p->d_rp, rp.data(), rp.size() * 4);
+  up((void**)&p->d_cols, cols.data(), cols.size() * 4);
+  up((void**)&p->d_goff, goff.data(), goff.size() * 4);
+  up((void**)&p->d_query, qv.data(), qv.size());
+  up((void**)&p->d_items, items.data(), items.size() * 8);
+  BCK(cudaMalloc((void**)&p->d_counts, num * sizeof(unsigned long long)));
+  BCK(cudaMalloc((void**)&p->d_next, sizeof(unsigned int)));
+  // scratch for the largest grid of any candidate configuration
+  int max_groups = 0;
+  for (int G : {4, 8, 16, 32})
+    for (int block : {128, 256, 512}) max_groups = std::max(max_groups, GridFor(p, G, block) * (block / G));
+  BCK(cudaMalloc((void**)&p->d_scratch, (size_t)max_groups * p->nbuf * p->cap * 4));
+  // autotune: time each candidate on the batch itself
+  int bestG = o.granularity == 2 ? 32 : 8, bestB = o.block_threads ? o.block_threads : 256;
+  if (o.autotune) {
+    float best = 1e30f;
+    for (int G : {4, 8, 16, 32})
+      for (int block : {128, 256, 512}) {
+        float ms = TimeConfig(p, G, block);
+        if (ms < best) {
+          best = ms;
+          bestG = G;
+          bestB = block;
+        }
+      }
+  }
+  p->G = bestG;
+  p->block = bestB;
+  p->grid = GridFor(p, bestG, bestB);
+  if (p->use_graph) {
+    BCK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    Reset(p);
+    Launch(p, p->G, p->block, p->grid);
+    BCK(cudaStreamEndCapture(p->stream, &p->graph));
+    BCK(cudaGraphInstantiate(&p->exec, p->graph, 0));
+  }
+  BCK(cudaStreamSynchronize(p->stream));
+}
+
+void Run(sme_batch_plan* p, uint64_t* counts, double* ms) {
+  BCK(cudaSetDevice(p->device));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, p->stream);
+  if (p->use_graph) {
+    BCK(cudaGraphLaunch(p->exec, p->stream));
+  } else {
+    Reset(p);
+    Launch(p, p->G, p->block, p->grid);
+  }
+  cudaEventRecord(e1, p->stream);
+  BCK(cudaMemcpyAsync(counts, p->d_counts, p->num * sizeof(uint64_t), cudaMemcpyDeviceToHost, p->stream));
+  BCK(cudaStreamSynchronize(p->stream));
+  BCK(cudaGetLastError());
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ms) *ms = t;
+}
+
+template <typename F>
+sme_status BGuard(F&& f) {
+  try {
+    f();
+    return SME_OK;
+  } catch (const Error& e) {
+    SetLastError(e.what());
+    return e.status;
+  } catch (const std::exception& e) {
+    SetLastError(e.what());
+    return SME_ERR_INVALID_ARG;
+  }
+}
+}  // namespace
 
 extern "C" {
+
 sme_status sme_batch_opts_default(sme_batch_opts* o) {
   if (!o) return SME_ERR_INVALID_ARG;
   *o = sme_batch_opts{};
@@ -9,14 +564,47 @@ sme_status sme_batch_opts_default(sme_batch_opts* o) {
   o->use_graph = 1;
   return SME_OK;
 }
-sme_status sme_batch_count(sme_graph* const*, const int32_t*, uint64_t, const sme_batch_opts*, uint64_t*) {
-  return SME_ERR_INVALID_ARG;
+
+sme_status sme_batch_prepare(sme_graph* const* graphs, const int32_t* queries, uint64_t num,
+                             const sme_batch_opts* opts, sme_batch_plan** out) {
+  if (!graphs || !queries || !out) return SME_ERR_INVALID_ARG;
+  return BGuard([&] {
+    sme_batch_opts o;
+    sme_batch_opts_default(&o);
+    if (opts) o = *opts;
+    std::unique_ptr<sme_batch_plan> p(new sme_batch_plan());
+    Prepare(graphs, queries, num, o, p.get());
+    *out = p.release();
+  });
 }
-sme_status sme_batch_prepare(sme_graph* const*, const int32_t*, uint64_t, const sme_batch_opts*,
-                             sme_batch_plan**) {
-  return SME_ERR_INVALID_ARG;
+
+sme_status sme_batch_run(sme_batch_plan* p, uint64_t* counts, double* ms) {
+  if (!p || !counts) return SME_ERR_INVALID_ARG;
+  return BGuard([&] { Run(p, counts, ms); });
 }
-sme_status sme_batch_run(sme_batch_plan*, uint64_t*, double*) { return SME_ERR_INVALID_ARG; }
-sme_status sme_batch_describe(const sme_batch_plan*, int32_t*, int32_t*, uint64_t*) { return SME_ERR_INVALID_ARG; }
-sme_status sme_batch_free(sme_batch_plan*) { return SME_OK; }
+
+sme_status sme_batch_describe(const sme_batch_plan* p, int32_t* g, int32_t* block, uint64_t* items) {
+  if (!p) return SME_ERR_INVALID_ARG;
+  if (g) *g = p->G;
+  if (block) *block = p->block;
+  if (items) *items = p->nitems;
+  return SME_OK;
 }
+
+sme_status sme_batch_free(sme_batch_plan* p) {
+  delete p;
+  return SME_OK;
+}
+
+sme_status sme_batch_count(sme_graph* const* graphs, const int32_t* queries, uint64_t num,
+                           const sme_batch_opts* opts, uint64_t* counts) {
+  if (!graphs || !queries || !counts) return SME_ERR_INVALID_ARG;
+  sme_batch_plan* p = nullptr;
+  sme_status st = sme_batch_prepare(graphs, queries, num, opts, &p);
+  if (st != SME_OK) return st;
+  st = sme_batch_run(p, counts, nullptr);
+  sme_batch_free(p);
+  return st;
+}
+
+}  // extern "C"

@@ -9,10 +9,6 @@
 #include "engine.h"
 #include "sme_internal.h"
 
-struct sme_graph {
-  sme::HostGraph g;
-};
-
 namespace sme {
 
 static thread_local std::string t_last_error;

@@ -44,13 +44,20 @@ __global__ void k_iota(uint32_t* out, uint32_t n, uint32_t start) {
 // Children estimate of an intersection step: the smallest list (the pivot
 // size), an upper bound of the candidate count (ThreadEstimatePathCount<MIN>,
 // CheckConstraintsCommon.cuh:161-189).
-__global__ void k_est_compute(DFront F, DStep s, const uintE* __restrict__ rp, uint64_t* est) {
+// With `sumdeg`, also the bytes of adjacency lists the path reads (external
+// mode: the subgraph a batch must load, EXTEstimateIntersectCost,
+// src/gpu/impl/light/ext/EXTLIGHTOrganizeBatch.cuh:11-53).
+__global__ void k_est_compute(DFront F, DStep s, const uintE* __restrict__ rp, uint64_t* est,
+                              uint64_t* sumdeg) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x) {
-    uint64_t m = ~0ULL;
+    uint64_t m = ~0ULL, sd = 0;
     for (int i = 0; i < s.nconn; ++i) {
       uint32_t v = F.inst[s.conn[i]][p];
-      m = min(m, (uint64_t)(rp[v + 1] - rp[v]));
+      uint64_t d = rp[v + 1] - rp[v];
+      m = min(m, d);
+      sd += d;
     }
+    if (sumdeg) sumdeg[p] = sd;
     if (s.reuse >= 0) {
       const uint32_t* ptr;
       uint32_t len;
@@ -156,16 +163,22 @@ __global__ void k_scan_apply(uint64_t* data, uint32_t n, const uint64_t* __restr
 // Batch boundaries: for threshold k, the first path whose inclusive cost
 // exceeds cost(start-1) + (k+1)*budget (SplitBatchKernel,
 // src/gpu/utils/batch/SplitBatch.cuh:38-87).  cost(p) = pf*(p+1) + cf*est_incl[p].
-__global__ void k_split(const uint64_t* __restrict__ incl, uint32_t P, uint32_t start, double pf,
-                        double cf, double budget, uint32_t K, uint64_t* out) {
+__global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __restrict__ incl2, uint32_t P,
+                        uint32_t start, double pf, double cf, double cg, double budget, uint32_t K,
+                        uint64_t* out) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
-  double c0 = start == 0 ? 0.0 : pf * (double)start + cf * (double)incl[start - 1];
+  auto cost = [&](uint32_t p) {  // inclusive cost of paths [0, p]
+    double c = pf * (double)(p + 1) + cf * (double)incl[p];
+    if (incl2) c += cg * (double)incl2[p];
+    return c;
+  };
+  double c0 = start == 0 ? 0.0 : cost(start - 1);
   double t = c0 + (double)(k + 1) * budget;
   uint32_t lo = start, hi = P;  // first p in [start,P) with cost(p) > t
   while (lo < hi) {
     uint32_t mid = lo + (hi - lo) / 2;
-    double c = pf * (double)(mid + 1) + cf * (double)incl[mid];
+    double c = cost(mid);
     if (c > t) hi = mid;
     else lo = mid + 1;
   }
@@ -506,6 +519,55 @@ __global__ void k_count_direct(DFront F, uint8_t nu, uint8_t u0, uint8_t u1, uin
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(acc, s);
 }
 
+// ---- external mode: per-batch subgraph ------------------------------------
+// Marks the adjacency lists a batch's intersections read
+// (InspectRequiredAdjLists, src/gpu/impl/common/ext/EXTGraphGPUCommon.cuh:157-184).
+__global__ void k_ext_mark(DFront F, DStep s, uint8_t* flag) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x)
+    for (int i = 0; i < s.nconn; ++i) flag[F.inst[s.conn[i]][p]] = 1;
+}
+
+// Degree of each required vertex (0 elsewhere) and the required flag, for the
+// subgraph's global-id row pointers (BuildSubgraphRowPtrs, EXTGraphGPUCommon.cuh:26-55).
+__global__ void k_ext_deg(const uint8_t* __restrict__ flag, const uintE* __restrict__ rp, uint32_t n,
+                          uint64_t* deg, uint64_t* fl) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    bool f = flag[v] != 0;
+    deg[v] = f ? rp[v + 1] - rp[v] : 0;
+    fl[v] = f ? 1 : 0;
+  }
+}
+
+__global__ void k_ext_rowptr(const uint64_t* __restrict__ deg_incl, uint32_t n, uintE* sub_rp) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x)
+    sub_rp[v] = v == 0 ? 0 : deg_incl[v - 1];
+}
+
+__global__ void k_ext_ids(const uint8_t* __restrict__ flag, const uint64_t* __restrict__ fl_incl, uint32_t n,
+                          uint32_t* ids) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    if (flag[v]) ids[fl_incl[v] - 1] = v;
+}
+
+// Copies the required lists from pinned, mapped host memory into the device
+// subgraph (one warp per list, coalesced reads over the host link); replaces
+// the host-thread gather + synchronous H2D of LoadSubgraph
+// (src/gpu/impl/common/ext/LoadSubgraph.h:10-42, EXTGraphGPUCommon.cuh:60-149).
+__global__ void __launch_bounds__(WARP_BLOCK) k_ext_gather(const uint32_t* __restrict__ ids, uint32_t nid,
+                                                           const uintE* __restrict__ rp,
+                                                           const uint32_t* __restrict__ host_cols,
+                                                           const uintE* __restrict__ sub_rp,
+                                                           uint32_t* __restrict__ sub_cols) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < nid; i += nw) {
+    uint32_t v = ids[i];
+    uintE b = rp[v], e = rp[v + 1], o = sub_rp[v];
+    for (uintE j = b + lane; j < e; j += 32) sub_cols[o + (j - b)] = host_cols[j];
+  }
+}
+
 // Writes complete instances (all vertices materialised), in output slots.
 __global__ void k_emit(DFront F, uint8_t n, const uint8_t* __restrict__ slot_dummy, uint8_t s0,
                        uint8_t s1, uint8_t s2, uint8_t s3, uint8_t s4, uint8_t s5, uint32_t* out,
@@ -649,10 +711,22 @@ class Executor {
     sms_ = SmCount(ctx.device);
   }
 
+  // External mode: adjacency lists are read from `host_cols` (pinned and
+  // mapped host memory) into a per-batch device subgraph; g_.row_ptrs holds
+  // the global row pointers on the device (GraphDevTracker,
+  // src/gpu/graph/GraphDevTracker.cuh:12-79).
+  void SetExternal(const uint32_t* host_cols) { ext_cols_ = host_cols; }
+  uint64_t ext_h2d_bytes() const { return ext_bytes_; }
+  uint64_t ext_loads() const { return ext_loads_; }
+
   RunResult Run(uint64_t rb, uint64_t re) {
     auto t0 = std::chrono::steady_clock::now();
     size_t mark = A_.Mark();
     ctrl_ = (unsigned long long*)A_.Alloc(8 * sizeof(unsigned long long));
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    CK(cudaEventRecord(ev0, st_));
     CK(cudaMemsetAsync(ctrl_, 0, 8 * sizeof(unsigned long long), st_));
     const Step& s0 = prog_.steps[0];
     const uint64_t R = re > rb ? re - rb : 0;
@@ -674,9 +748,14 @@ class Executor {
       A_.Release(m);
     }
     (void)R;
+    CK(cudaEventRecord(ev1, st_));
     unsigned long long h[8];
     CK(cudaMemcpyAsync(h, ctrl_, sizeof(h), cudaMemcpyDeviceToHost, st_));
     CK(cudaStreamSynchronize(st_));
+    float dev_ms = 0;
+    cudaEventElapsedTime(&dev_ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
     CK(cudaGetLastError());
     if (h[3]) Fail(SME_ERR_CUDA, "device bounds check failed (engine error flags " + std::to_string(h[3]) + ")");
     RunResult r;
@@ -697,6 +776,8 @@ class Executor {
     }
     events_.clear();
     r.stats.kernel_ms = ms_total;
+    r.stats.device_ms = dev_ms;
+    r.stats.hot_launches = hot_;
     r.stats.elapsed_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     A_.Release(mark);
@@ -713,7 +794,52 @@ class Executor {
   uint64_t cap_;
   int sms_ = 148;
   unsigned long long* ctrl_ = nullptr;  // [0] count [1] bytes [2] emitted [3] error flags
-  uint64_t launches_ = 0, batches_ = 0, paths_ = 0;
+  uint64_t launches_ = 0, batches_ = 0, paths_ = 0, hot_ = 0;
+  const uint32_t* ext_cols_ = nullptr;
+  uint64_t ext_bytes_ = 0, ext_loads_ = 0;
+
+  struct GraphView {
+    const uintE* rp;
+    const uint32_t* cols;
+  };
+
+  // Loads, for the paths of Fb, the adjacency lists step `ds` intersects into
+  // a device subgraph allocated in the current arena frame (it stays valid
+  // while deeper levels use candidate sets that point into it).
+  GraphView LoadSubgraph(const DFront& Fb, const DStep& ds) {
+    if (!ext_cols_) return GraphView{g_.row_ptrs, g_.cols};
+    const uint32_t n = (uint32_t)g_.n;
+    const size_t mark = A_.Mark();
+    uint8_t* flag = (uint8_t*)A_.Alloc(n);
+    uint64_t* deg = (uint64_t*)A_.Alloc((size_t)n * 8);
+    uint64_t* fl = (uint64_t*)A_.Alloc((size_t)n * 8);
+    CK(cudaMemsetAsync(flag, 0, n, st_));
+    k_ext_mark<<<Grid(Fb.P, 256), 256, 0, st_>>>(Fb, ds, flag);
+    k_ext_deg<<<Grid(n, 256), 256, 0, st_>>>(flag, g_.row_ptrs, n, deg, fl);
+    launches_ += 2;
+    Scan(deg, n);
+    Scan(fl, n);
+    CK(cudaMemcpyAsync(ctx_.h_pinned, deg + n - 1, 8, cudaMemcpyDeviceToHost, st_));
+    CK(cudaMemcpyAsync(ctx_.h_pinned + 1, fl + n - 1, 8, cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    const uint64_t sub_m = ctx_.h_pinned[0], nid = ctx_.h_pinned[1];
+    // keep the subgraph below the scratch: release the scratch by rebuilding
+    // the frame as [sub_rp, sub_cols, ids] and recomputing from the scans
+    uint64_t* deg_keep = deg;
+    uint64_t* fl_keep = fl;
+    uintE* sub_rp = (uintE*)A_.Alloc((size_t)(n + 1) * 8);
+    uint32_t* sub_cols = (uint32_t*)A_.Alloc(std::max<uint64_t>(sub_m, 1) * 4);
+    uint32_t* ids = (uint32_t*)A_.Alloc(std::max<uint64_t>(nid, 1) * 4);
+    k_ext_rowptr<<<Grid(n + 1, 256), 256, 0, st_>>>(deg_keep, n, sub_rp);
+    k_ext_ids<<<Grid(n, 256), 256, 0, st_>>>(flag, fl_keep, n, ids);
+    k_ext_gather<<<WarpGrid(nid), WARP_BLOCK, 0, st_>>>(ids, (uint32_t)nid, g_.row_ptrs, ext_cols_, sub_rp,
+                                                         sub_cols);
+    launches_ += 3;
+    ext_bytes_ += sub_m * 4;
+    ++ext_loads_;
+    (void)mark;
+    return GraphView{sub_rp, sub_cols};
+  }
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events_;
 
   void Launched() { ++launches_; }
@@ -739,6 +865,7 @@ class Executor {
   void TimerStop(std::pair<cudaEvent_t, cudaEvent_t> e) {
     cudaEventRecord(e.second, st_);
     events_.push_back(e);
+    ++hot_;
   }
 
   void Scan(uint64_t* d, uint32_t n) {
@@ -764,7 +891,8 @@ class Executor {
     uint64_t e0, e1;  // inclusive estimate before b0 / at b1-1
   };
 
-  std::vector<Batch> Split(const uint64_t* incl, uint32_t P, double pf, double cf, uint64_t budget) {
+  std::vector<Batch> Split(const uint64_t* incl, uint32_t P, double pf, double cf, uint64_t budget,
+                           const uint64_t* incl2 = nullptr, double cg = 0) {
     std::vector<Batch> out;
     if (P == 0) return out;
     budget = std::max<uint64_t>(budget, 1 << 20);
@@ -774,7 +902,7 @@ class Executor {
     uint32_t start = 0;
     uint64_t e_start = 0;
     while (start < P) {
-      k_split<<<(K + 255) / 256, 256, 0, st_>>>(incl, P, start, pf, cf, (double)budget, K, d);
+      k_split<<<(K + 255) / 256, 256, 0, st_>>>(incl, incl2, P, start, pf, cf, cg, (double)budget, K, d);
       Launched();
       CK(cudaMemcpyAsync(ctx_.h_pinned, d, (size_t)K * 16, cudaMemcpyDeviceToHost, st_));
       CK(cudaStreamSynchronize(st_));
@@ -824,11 +952,35 @@ class Executor {
     switch (s.kind) {
       case S_COMPUTE_COUNT: {
         paths_ += F.P;
-        auto t = TimerStart();
-        k_compute<1><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, g_.row_ptrs, g_.cols, nullptr, 0,
-                                                            nullptr, nullptr, nullptr, 0, acc, err);
-        TimerStop(t);
+        if (!ext_cols_) {
+          auto t = TimerStart();
+          k_compute<1><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, g_.row_ptrs, g_.cols, nullptr, 0,
+                                                              nullptr, nullptr, nullptr, 0, acc, err);
+          TimerStop(t);
+          Launched();
+          return;
+        }
+        // external: batches whose required lists fit the level budget
+        const size_t m0 = A_.Mark();
+        uint64_t* est = (uint64_t*)A_.Alloc((size_t)F.P * 8);
+        uint64_t* sd = (uint64_t*)A_.Alloc((size_t)F.P * 8);
+        k_est_compute<<<Grid(F.P, 256), 256, 0, st_>>>(F, ds, g_.row_ptrs, est, sd);
         Launched();
+        Scan(sd, F.P);
+        std::vector<Batch> bs = Split(sd, F.P, 0.0, 4.0 + 8.0, Budget(k));
+        for (const Batch& b : bs) {
+          const size_t mk = A_.Mark();
+          DFront Fb = Slice(F, b.b0, b.b1);
+          ++batches_;
+          GraphView gv = LoadSubgraph(Fb, ds);
+          auto t = TimerStart();
+          k_compute<1><<<WarpGrid(Fb.P), WARP_BLOCK, 0, st_>>>(Fb, ds, gv.rp, gv.cols, nullptr, 0, nullptr,
+                                                               nullptr, nullptr, 0, acc, err);
+          TimerStop(t);
+          Launched();
+          A_.Release(mk);
+        }
+        A_.Release(m0);
         return;
       }
       case S_COUNT: {
@@ -850,9 +1002,11 @@ class Executor {
     }
     const size_t mark0 = A_.Mark();
     uint64_t* est = (uint64_t*)A_.Alloc((size_t)F.P * 8);
+    uint64_t* sumdeg = nullptr;  // external mode: subgraph bytes per path
     double pf = 0, cf = 0;
     if (s.kind == S_COMPUTE || s.kind == S_PATH_COUNT) {
-      k_est_compute<<<Grid(F.P, 256), 256, 0, st_>>>(F, ds, g_.row_ptrs, est);
+      if (ext_cols_) sumdeg = (uint64_t*)A_.Alloc((size_t)F.P * 8);
+      k_est_compute<<<Grid(F.P, 256), 256, 0, st_>>>(F, ds, g_.row_ptrs, est, sumdeg);
       pf = 12 + 16;
       cf = s.kind == S_COMPUTE ? 4 : 0;
     } else {  // MATERIALIZE, FILTER
@@ -867,10 +1021,11 @@ class Executor {
     }
     Launched();
     Scan(est, F.P);
+    if (sumdeg) Scan(sumdeg, F.P);
     uint64_t budget = Budget(k);
     // keep child counts of a batch within 31-bit path indices
     budget = std::min<uint64_t>(budget, (uint64_t)(std::max(cf, 1.0) * 2.0e9));
-    std::vector<Batch> batches = Split(est, F.P, pf, cf, budget);
+    std::vector<Batch> batches = Split(est, F.P, pf, cf, budget, sumdeg, 4.0 + 8.0);
     for (const Batch& b : batches) {
       const size_t mark = A_.Mark();
       DFront Fb = Slice(F, b.b0, b.b1);
@@ -884,12 +1039,13 @@ class Executor {
           uint32_t* cnt = (uint32_t*)A_.Alloc((size_t)Pb * 4);
           uint64_t cap = s.kind == S_COMPUTE ? b.e1 - b.e0 : 0;
           uint32_t* data = cap ? (uint32_t*)A_.Alloc(cap * 4) : nullptr;
+          GraphView gv = LoadSubgraph(Fb, ds);
           auto t = TimerStart();
           if (s.kind == S_COMPUTE)
-            k_compute<0><<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, ds, g_.row_ptrs, g_.cols, est, b.b0, ptr,
+            k_compute<0><<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, ds, gv.rp, gv.cols, est, b.b0, ptr,
                                                                cnt, data, cap, acc, err);
           else
-            k_compute<2><<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, ds, g_.row_ptrs, g_.cols, est, b.b0, ptr,
+            k_compute<2><<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, ds, gv.rp, gv.cols, est, b.b0, ptr,
                                                                cnt, nullptr, 0, acc, err);
           TimerStop(t);
           Launched();
@@ -970,6 +1126,70 @@ RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& c
   if (rb > re) rb = re;
   Executor ex(prog, g, ctx, d_out, cap);
   return ex.Run(rb, re);
+}
+
+// EXTERNAL_GPU: the graph stays in host memory.
+//   EXT_CACHE  global row pointers on the device; for every intersection
+//              batch, the required adjacency lists are gathered by the GPU
+//              from pinned, mapped host memory into a device subgraph
+//              (EXTLIGHTGPUProcessor::PrepareBatch/LoadSubgraph,
+//              src/gpu/impl/light/ext/EXTLIGHTGPUProcessor.cuh:20-90).
+//   EXT_UMA    the adjacency lists live in managed memory and migrate on
+//              demand (EXTUMALIGHTGPUComp, src/gpu/impl/light/ext/uma/).
+RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceContext& ctx, uint64_t rb,
+                             uint64_t re, int ext_variant, uint64_t graph_budget_bytes) {
+  (void)graph_budget_bytes;
+  CK(cudaSetDevice(ctx.device));
+  if (re > hg.n) re = hg.n;
+  if (rb > re) rb = re;
+  DeviceGraph dg;
+  dg.device = ctx.device;
+  dg.n = hg.n;
+  dg.m = hg.m;
+  uint64_t h2d = (hg.n + 1) * sizeof(uintE);
+  CK(cudaMalloc((void**)&dg.row_ptrs, (hg.n + 1) * sizeof(uintE)));
+  RunResult r;
+  bool registered = false;
+  uint32_t* managed = nullptr;
+  try {
+    CK(cudaMemcpyAsync(dg.row_ptrs, hg.row_ptrs, (hg.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, ctx.stream));
+    if (ext_variant == SME_EXT_UMA) {
+      CK(cudaMallocManaged((void**)&managed, std::max<uint64_t>(hg.m, 1) * sizeof(uintV)));
+      if (hg.m) std::memcpy(managed, hg.cols, hg.m * sizeof(uintV));
+      dg.cols = managed;
+      Executor ex(prog, dg, ctx, nullptr, 0);
+      r = ex.Run(rb, re);
+      h2d += hg.m * sizeof(uintV);
+    } else {
+      const uint32_t* dcols = nullptr;
+      if (hg.m) {
+        cudaError_t e = cudaHostRegister(hg.cols, hg.m * sizeof(uintV), cudaHostRegisterMapped | cudaHostRegisterReadOnly);
+        if (e == cudaSuccess) {
+          registered = true;
+        } else if (e == cudaErrorHostMemoryAlreadyRegistered) {
+          cudaGetLastError();
+        } else {
+          Fail(SME_ERR_CUDA, std::string("cudaHostRegister: ") + cudaGetErrorString(e));
+        }
+        CK(cudaHostGetDevicePointer((void**)&dcols, hg.cols, 0));
+      }
+      Executor ex(prog, dg, ctx, nullptr, 0);
+      ex.SetExternal(dcols);
+      r = ex.Run(rb, re);
+      h2d += ex.ext_h2d_bytes();
+    }
+  } catch (...) {
+    cudaStreamSynchronize(ctx.stream);
+    if (registered) cudaHostUnregister(hg.cols);
+    if (managed) cudaFree(managed);
+    cudaFree(dg.row_ptrs);
+    throw;
+  }
+  if (registered) cudaHostUnregister(hg.cols);
+  if (managed) cudaFree(managed);
+  cudaFree(dg.row_ptrs);
+  r.stats.h2d_bytes = h2d;
+  return r;
 }
 
 }  // namespace sme

@@ -1,21 +1,280 @@
-// Served form: placeholder.
-#include "../../include/sme.h"
+// Served form: a request loop over device-resident graphs with admission by
+// estimated frontier memory and continuous batching across slots.
+//
+// Each slot owns a CUDA stream and a frontier arena, and a host worker that
+// runs one request at a time through the level engine; requests of different
+// patterns and graphs therefore run concurrently on the device.  A request is
+// admitted when a slot is idle and the sum of the estimated frontier bytes of
+// the requests in flight stays within the server budget; otherwise it waits
+// in the FIFO queue (the head is never overtaken, so no request starves).
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "engine.h"
+#include "sme_internal.h"
+
+namespace sme {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t id;
+  int32_t gid;
+  sme_graph* attached;
+  sme_opts opts;
+  uint64_t est_bytes;
+  Clock::time_point submitted;
+};
+
+struct Result {
+  sme_status status = SME_ERR_BUSY;
+  uint64_t count = 0;
+  double latency_ms = 0;
+  std::string error;
+};
+
+// Frontier estimate of a request: the partial instances of the widest level
+// are bounded by the edge count times the pattern's later levels; the engine
+// batches to its slot arena, so the estimate only orders admission.
+uint64_t EstimateBytes(const HostGraph& g, int query) {
+  const int k = Query(query).n;
+  uint64_t graph = (g.n + 1) * 8 + g.m * 4;
+  uint64_t frontier = g.m * 4ULL * (uint64_t)std::max(1, k - 2) * 4ULL;
+  return graph + frontier;
+}
+
+}  // namespace
+}  // namespace sme
+
+using namespace sme;
+
+struct sme_server {
+  sme_server_opts o{};
+  std::vector<sme_graph*> resident;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request> queue;
+  std::map<uint64_t, Result> results;
+  std::vector<std::thread> workers;
+  std::vector<DeviceContext*> ctxs;
+  uint64_t next_id = 1;
+  uint64_t inflight_bytes = 0;
+  uint64_t inflight = 0, max_inflight = 0, completed = 0, rejected = 0;
+  bool stop = false;
+  uint64_t slot_arena = 0;
+
+  void Worker(int slot) {
+    cudaSetDevice(o.device);
+    DeviceContext* ctx = ctxs[slot];
+    while (true) {
+      Request r;
+      {
+        std::unique_lock<std::mutex> l(mu);
+        cv_work.wait(l, [&] {
+          return stop || (!queue.empty() && (inflight == 0 || inflight_bytes + queue.front().est_bytes <=
+                                                                   o.mem_budget_bytes));
+        });
+        if (stop && queue.empty()) return;
+        r = queue.front();
+        queue.pop_front();
+        inflight_bytes += r.est_bytes;
+        ++inflight;
+        max_inflight = std::max(max_inflight, inflight);
+      }
+      Result res;
+      try {
+        const HostGraph& hg = r.attached ? r.attached->g : resident[r.gid]->g;
+        Program prog = Compile(r.opts, false);
+        DeviceGraph* dg = hg.dev;
+        bool temp = false;
+        if (!dg || dg->device != o.device) {
+          dg = UploadGraph(hg, o.device, ctx->stream, nullptr);
+          temp = true;
+        }
+        uint64_t re = r.opts.root_end ? std::min<uint64_t>(r.opts.root_end, hg.n) : hg.n;
+        RunResult rr;
+        try {
+          rr = RunProgram(prog, *dg, *ctx, r.opts.root_begin, re, nullptr, 0, 0);
+        } catch (...) {
+          if (temp) FreeDeviceGraph(dg);
+          throw;
+        }
+        if (temp) FreeDeviceGraph(dg);
+        res.status = SME_OK;
+        res.count = rr.count;
+      } catch (const Error& e) {
+        res.status = e.status;
+        res.error = e.what();
+      } catch (const std::exception& e) {
+        res.status = SME_ERR_INVALID_ARG;
+        res.error = e.what();
+      }
+      res.latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - r.submitted).count();
+      {
+        std::lock_guard<std::mutex> l(mu);
+        results[r.id] = res;
+        inflight_bytes -= r.est_bytes;
+        --inflight;
+        ++completed;
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+  }
+};
+
+namespace {
+template <typename F>
+sme_status SGuard(F&& f) {
+  try {
+    f();
+    return SME_OK;
+  } catch (const Error& e) {
+    SetLastError(e.what());
+    return e.status;
+  } catch (const std::exception& e) {
+    SetLastError(e.what());
+    return SME_ERR_INVALID_ARG;
+  }
+}
+}  // namespace
 
 extern "C" {
+
 sme_status sme_server_opts_default(sme_server_opts* o) {
   if (!o) return SME_ERR_INVALID_ARG;
   *o = sme_server_opts{};
+  o->device = 0;
   o->slots = 4;
-  o->queue_capacity = 4096;
+  o->mem_budget_bytes = 0;  // 0: 60% of free device memory
+  o->queue_capacity = 1 << 16;
   return SME_OK;
 }
-sme_status sme_server_create(const sme_server_opts*, sme_server**) { return SME_ERR_INVALID_ARG; }
-sme_status sme_server_add_graph(sme_server*, sme_graph*, int32_t*) { return SME_ERR_INVALID_ARG; }
-sme_status sme_server_submit(sme_server*, int32_t, sme_graph*, const sme_opts*, uint64_t*) {
-  return SME_ERR_INVALID_ARG;
+
+sme_status sme_server_create(const sme_server_opts* opts, sme_server** out) {
+  if (!out) return SME_ERR_INVALID_ARG;
+  return SGuard([&] {
+    std::unique_ptr<sme_server> s(new sme_server());
+    sme_server_opts_default(&s->o);
+    if (opts) s->o = *opts;
+    if (s->o.slots < 1 || s->o.slots > 64) Fail(SME_ERR_INVALID_ARG, "slots must be 1..64");
+    if (DeviceCount() <= s->o.device) Fail(SME_ERR_NO_DEVICE, "no CUDA device " + std::to_string(s->o.device));
+    cudaSetDevice(s->o.device);
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    if (!s->o.mem_budget_bytes) s->o.mem_budget_bytes = (uint64_t)(fr * 0.6);
+    s->slot_arena = std::max<uint64_t>(s->o.mem_budget_bytes / s->o.slots, 256ULL << 20);
+    for (int i = 0; i < s->o.slots; ++i) s->ctxs.push_back(CreateContext(s->o.device, s->slot_arena));
+    for (int i = 0; i < s->o.slots; ++i) s->workers.emplace_back(&sme_server::Worker, s.get(), i);
+    *out = s.release();
+  });
 }
-sme_status sme_server_poll(sme_server*, uint64_t, uint64_t*, double*) { return SME_ERR_INVALID_ARG; }
-sme_status sme_server_wait(sme_server*, uint64_t, uint64_t*, double*) { return SME_ERR_INVALID_ARG; }
-sme_status sme_server_stats(sme_server*, uint64_t*, uint64_t*, uint64_t*) { return SME_ERR_INVALID_ARG; }
-sme_status sme_server_destroy(sme_server*) { return SME_OK; }
+
+sme_status sme_server_add_graph(sme_server* s, sme_graph* g, int32_t* gid) {
+  if (!s || !g || !gid) return SME_ERR_INVALID_ARG;
+  return SGuard([&] {
+    if (!g->g.dev || g->g.dev->device != s->o.device) {
+      if (g->g.dev) FreeDeviceGraph(g->g.dev);
+      g->g.dev = nullptr;
+      cudaSetDevice(s->o.device);
+      g->g.dev = UploadGraph(g->g, s->o.device, 0, nullptr);
+    }
+    std::lock_guard<std::mutex> l(s->mu);
+    s->resident.push_back(g);
+    *gid = (int32_t)s->resident.size() - 1;
+  });
 }
+
+sme_status sme_server_submit(sme_server* s, int32_t gid, sme_graph* attached, const sme_opts* opts,
+                             uint64_t* request_id) {
+  if (!s || !opts || !request_id) return SME_ERR_INVALID_ARG;
+  return SGuard([&] {
+    if (opts->execute_mode != SME_IN_MEMORY_GPU) Fail(SME_ERR_INVALID_ARG, "served requests run IN_MEMORY_GPU");
+    Request r;
+    r.gid = gid;
+    r.attached = attached;
+    r.opts = *opts;
+    r.opts.device = s->o.device;
+    r.submitted = Clock::now();
+    {
+      std::lock_guard<std::mutex> l(s->mu);
+      if (!attached && (gid < 0 || gid >= (int32_t)s->resident.size()))
+        Fail(SME_ERR_INVALID_ARG, "unknown graph id " + std::to_string(gid));
+      if ((int64_t)s->queue.size() >= s->o.queue_capacity) {
+        ++s->rejected;
+        Fail(SME_ERR_BUSY, "server queue full");
+      }
+      const HostGraph& hg = attached ? attached->g : s->resident[gid]->g;
+      Compile(r.opts, false);  // validate query / plan before queueing
+      r.est_bytes = EstimateBytes(hg, r.opts.query_type);
+      r.id = s->next_id++;
+      s->results[r.id] = Result();
+      s->queue.push_back(r);
+      *request_id = r.id;
+    }
+    s->cv_work.notify_one();
+  });
+}
+
+sme_status sme_server_poll(sme_server* s, uint64_t id, uint64_t* count, double* latency_ms) {
+  if (!s) return SME_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> l(s->mu);
+  auto it = s->results.find(id);
+  if (it == s->results.end()) {
+    SetLastError("unknown request id");
+    return SME_ERR_INVALID_ARG;
+  }
+  if (it->second.status == SME_ERR_BUSY) return SME_ERR_BUSY;
+  if (count) *count = it->second.count;
+  if (latency_ms) *latency_ms = it->second.latency_ms;
+  if (it->second.status != SME_OK) SetLastError(it->second.error);
+  return it->second.status;
+}
+
+sme_status sme_server_wait(sme_server* s, uint64_t id, uint64_t* count, double* latency_ms) {
+  if (!s) return SME_ERR_INVALID_ARG;
+  std::unique_lock<std::mutex> l(s->mu);
+  auto it = s->results.find(id);
+  if (it == s->results.end()) {
+    SetLastError("unknown request id");
+    return SME_ERR_INVALID_ARG;
+  }
+  s->cv_done.wait(l, [&] { return s->results[id].status != SME_ERR_BUSY; });
+  const Result& r = s->results[id];
+  if (count) *count = r.count;
+  if (latency_ms) *latency_ms = r.latency_ms;
+  if (r.status != SME_OK) SetLastError(r.error);
+  return r.status;
+}
+
+sme_status sme_server_stats(sme_server* s, uint64_t* completed, uint64_t* max_inflight, uint64_t* rejected) {
+  if (!s) return SME_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> l(s->mu);
+  if (completed) *completed = s->completed;
+  if (max_inflight) *max_inflight = s->max_inflight;
+  if (rejected) *rejected = s->rejected;
+  return SME_OK;
+}
+
+sme_status sme_server_destroy(sme_server* s) {
+  if (!s) return SME_OK;
+  {
+    std::lock_guard<std::mutex> l(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  for (auto& t : s->workers) t.join();
+  for (auto* c : s->ctxs) DestroyContext(c);
+  delete s;
+  return SME_OK;
+}
+
+}  // extern "C"

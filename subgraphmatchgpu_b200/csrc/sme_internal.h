@@ -183,3 +183,8 @@ struct Program {
 Program Compile(const sme_opts& o, bool enumerate);
 
 }  // namespace sme
+
+// Opaque handle of the C-ABI (include/sme.h).
+struct sme_graph {
+  sme::HostGraph g;
+};

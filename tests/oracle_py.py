@@ -25,6 +25,9 @@ def lib():
                                   C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]
         L.oracle_query_size.restype = C.c_int
         L.oracle_query_size.argtypes = [C.c_int]
+        L.oracle_wcoj_strided.restype = C.c_uint64
+        L.oracle_wcoj_strided.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_uint64,
+                                          C.c_uint64, C.c_int]
         _lib = L
     return _lib
 
@@ -34,6 +37,13 @@ def count(row_ptrs, cols, q, ordering=True, root_begin=0, root_end=0, threads=0)
     cl = np.ascontiguousarray(cols, dtype=np.uint32)
     return int(lib().oracle_wcoj(rp.ctypes.data, cl.ctypes.data if len(cl) else None, len(rp) - 1, q,
                                  int(ordering), root_begin, root_end, threads, None, 0, None))
+
+
+def count_strided(row_ptrs, cols, q, stride, offset=0, threads=0, ordering=True) -> int:
+    rp = np.ascontiguousarray(row_ptrs, dtype=np.uint64)
+    cl = np.ascontiguousarray(cols, dtype=np.uint32)
+    return int(lib().oracle_wcoj_strided(rp.ctypes.data, cl.ctypes.data if len(cl) else None, len(rp) - 1, q,
+                                         int(ordering), stride, offset, threads))
 
 
 def enumerate_sorted(row_ptrs, cols, q, ordering=True) -> np.ndarray:
