@@ -46,9 +46,13 @@ def parse():
     ap.add_argument("--queries", default="3,1,2")
     ap.add_argument("--algo", type=int, default=6)
     ap.add_argument("--tasks", type=int, default=2, help="root-range tasks per query")
+    ap.add_argument("--q1-stride", type=int, default=1024, help="4-cycle: roots per strided task = n/stride")
+    ap.add_argument("--q1-tasks", type=int, default=3, help="4-cycle: strided tasks in the step cycle")
     ap.add_argument("--root-end", type=int, default=0, help="restrict roots to [0, root_end) (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--granularity", type=int, default=0, help="0 auto, 1 warp per path, 2 flattened")
+    ap.add_argument("--list-only", action="store_true", help="no hub bitmaps (comparison)")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
@@ -110,10 +114,21 @@ def make_graph(args):
 
 
 def work_items(args, n):
+    """(query, root_begin, root_end, root_stride) tasks.  Queries whose full
+    count fits a few seconds (4-clique, diamond) use `tasks` contiguous root
+    ranges; the 4-cycle, whose full count at this scale takes minutes, uses
+    strided tasks (every `q1_stride`-th root from offset k), each an unbiased
+    1/q1_stride slice of the roots."""
     qs = [int(q) for q in args.queries.split(",")]
     end = args.root_end or n
-    cuts = [end * i // args.tasks for i in range(args.tasks + 1)]
-    return [(q, a, b) for q in qs for a, b in zip(cuts, cuts[1:])]
+    items = []
+    for q in qs:
+        if q == 1 and not args.root_end:
+            items += [(q, k, end, args.q1_stride) for k in range(args.q1_tasks)]
+        else:
+            cuts = [end * i // args.tasks for i in range(args.tasks + 1)]
+            items += [(q, a, b, 1) for a, b in zip(cuts, cuts[1:])]
+    return items
 
 
 def load_traffic():
@@ -141,26 +156,22 @@ def cpu_baseline(g, items, budget_s):
     rp, cl = g.csr()
     n = len(rp) - 1
     threads = os.cpu_count() or 1
-    qs = sorted({q for q, _, _ in items})
-    # strided root sample (roots r with r % stride == offset: hubs and tail
-    # alike); a coarse probe calibrates the stride to about budget_s seconds
-    offset = 1
-    stride = max(1, n // 64)
-    t0 = time.perf_counter()
+    import numpy as np
+    qs = sorted({it[0] for it in items})
+    # roots in a seeded random order (hubs and tail alike), processed until the
+    # per-query share of the budget runs out; roots cut short are discarded
+    roots = np.random.default_rng(12345).permutation(n).astype(np.uint32)
+    total_inst, total_t, done = 0, 0.0, {}
     for q in qs:
-        O.count_strided(rp, cl, q, stride, offset, threads)
-    probe = time.perf_counter() - t0
-    if probe < budget_s / 2:
-        stride = max(1, int(stride * probe / budget_s))
-    total_inst = 0
-    t0 = time.perf_counter()
-    for q in qs:
-        total_inst += O.count_strided(rp, cl, q, stride, offset, threads)
-    total_t = time.perf_counter() - t0
+        inst, d, t = O.count_sample(rp, cl, q, roots, budget_s / len(qs), threads)
+        total_inst += inst
+        total_t += t
+        done[q] = d
     return {"value": total_inst / total_t if total_t > 0 else 0.0, "unit": UNIT, "cores": threads,
             "kind": "port",
-            "sample": f"roots r with r % {stride} == {offset} of the same R-MAT graph ({(n + stride - 1) // stride} "
-                      f"roots), queries {qs}: {total_inst} instances in {total_t:.2f}s"}, total_inst, total_t
+            "sample": f"CPU_WCOJ port, {threads} threads, roots of the same R-MAT graph in a seeded random order "
+                      f"until {budget_s / len(qs):.1f}s per query; completed roots per query {done}; "
+                      f"{total_inst} instances in {total_t:.2f}s"}, total_inst, total_t
 
 
 def run_reference(args, rank, world):
@@ -211,10 +222,11 @@ def main():
     n, m, dmax = g.info()
     g.to_device(local)
     items = work_items(args, n)
+    tune = {"warp_granularity": args.granularity, "list_only": int(args.list_only)}
 
     def step(i):
-        q, a, b = items[i % len(items)]
-        c = g.count(q, args.algo, root_begin=a, root_end=b, device=local)
+        q, a, b, st = items[i % len(items)]
+        c = g.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
         return c, sme.last_stats()
 
     for i in range(args.warmup):
@@ -259,12 +271,13 @@ def main():
         pcl = torch.from_numpy(cl).pin_memory()
         gh = sme.Graph.from_csr(prp.numpy(), pcl.numpy(), copy=False)
         e_inst, e_t, h2d, d2h = 0, 0.0, 0, 0
-        gh.count(items[0][0], args.algo, root_begin=items[0][1], root_end=items[0][2], device=local)
+        q, a, b, st = items[-1]
+        gh.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
         for i in range(args.steps):
-            q, a, b = items[(args.warmup + i) % len(items)]
+            q, a, b, st = items[(args.warmup + i) % len(items)]
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            e_inst += gh.count(q, args.algo, root_begin=a, root_end=b, device=local)
+            e_inst += gh.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
             e_t += time.perf_counter() - t0
             s = sme.last_stats()
             h2d += s.h2d_bytes

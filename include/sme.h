@@ -76,8 +76,12 @@ typedef struct sme_opts {
   uint64_t mem_limit_bytes;/* device budget for frontiers+graph; 0 = auto    */
   uint64_t root_begin;     /* first-level vertex range [begin,end) (a task   */
   uint64_t root_end;       /*  of IntraPartScheduler); end==0 means all      */
-  int32_t warp_granularity;/* 0 auto, 1 warp per path only (tuning knob)     */
-  int32_t reserved[7];
+  int32_t warp_granularity;/* 0 auto (flattened), 1 warp per path, 2 flattened */
+  int32_t list_only;       /* 1: membership by binary search only, no hub
+                              bitmaps (comparison knob)                      */
+  uint32_t root_stride;    /* roots are root_begin, +stride, ... < root_end
+                              (0 or 1: every root); a strided task          */
+  int32_t reserved[5];
 } sme_opts;
 
 /* Counters of the last sme_count/sme_enumerate call on this thread. */

@@ -178,7 +178,18 @@ typedef struct {
   uint32_t* out;     /* optional instance output */
   uint64_t cap;
   uint64_t* pos;     /* shared output cursor */
+  double deadline;   /* omp_get_wtime() limit of a time-bounded sample (0: none) */
+  int* aborted;      /* set when the deadline cut a root short (per thread) */
 } ctx_t;
+
+static int expired(const ctx_t* c) {
+#ifdef _OPENMP
+  return c->deadline > 0 && omp_get_wtime() > c->deadline;
+#else
+  (void)c;
+  return 0;
+#endif
+}
 
 /* two-pointer merge of sorted a and b into out; returns size */
 static uint64_t merge(const uint32_t* a, uint64_t na, const uint32_t* b, uint64_t nb, uint32_t* out) {
@@ -244,6 +255,10 @@ static uint64_t dfs(const ctx_t* c, int level, uint32_t* path, uint32_t* buf) {
     for (int k = 0; k < level && ok; ++k)
       if (path[k] == x) ok = 0;
     if (!ok) continue;
+    if (level <= 2 && c->aborted && expired(c)) {
+      *c->aborted = 1;
+      return ans;
+    }
     path[level] = x;
     ans += dfs(c, level + 1, path, next);
   }
@@ -332,5 +347,57 @@ uint64_t oracle_wcoj_strided(const uint64_t* rp, const uint32_t* cols, uint64_t 
     }
     free(buf);
   }
+  return total;
+}
+
+/*
+ * Time-bounded sample for the CPU baseline: roots[0..nroots) are processed
+ * (OpenMP dynamic schedule) until `budget_s` seconds have passed; a root the
+ * deadline cuts short is discarded.  Returns the instances of the completed
+ * roots; *done = completed roots, *elapsed = wall seconds spent.
+ */
+uint64_t oracle_wcoj_sample(const uint64_t* rp, const uint32_t* cols, uint64_t nv, int q, int ordering,
+                            const uint32_t* roots, uint64_t nroots, int threads, double budget_s,
+                            uint64_t* done, double* elapsed) {
+  pattern_t p;
+  if (build_pattern(q, &p)) return (uint64_t)-1;
+  plan_t pl;
+  make_plan(&p, ordering, &pl);
+  uint64_t pos = 0;
+  uint64_t maxd = max_degree(rp, nv);
+  size_t per_thread = (size_t)(3 * maxd + 3) * (size_t)(MAXQ + 1);
+  uint64_t total = 0, completed = 0;
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+  const double t0 = omp_get_wtime();
+#else
+  const double t0 = 0;
+#endif
+  const double deadline = t0 + budget_s;
+#pragma omp parallel reduction(+ : total, completed)
+  {
+    int aborted = 0;
+    ctx_t c = {rp, cols, nv, &pl, NULL, 0, &pos, deadline, &aborted};
+    uint32_t* buf = (uint32_t*)malloc(sizeof(uint32_t) * per_thread);
+    uint32_t path[MAXQ];
+#pragma omp for schedule(dynamic, 1)
+    for (long long k = 0; k < (long long)nroots; ++k) {
+      if (expired(&c)) continue;
+      aborted = 0;
+      path[0] = roots[k];
+      uint64_t a = dfs(&c, 1, path, buf);
+      if (!aborted) {
+        total += a;
+        completed += 1;
+      }
+    }
+    free(buf);
+  }
+#ifdef _OPENMP
+  if (elapsed) *elapsed = omp_get_wtime() - t0;
+#else
+  if (elapsed) *elapsed = 0;
+#endif
+  if (done) *done = completed;
   return total;
 }

@@ -87,7 +87,7 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
   uint64_t h2d = 0, d2h = 8;
   if (o.execute_mode == SME_EXTERNAL_GPU) {
     if (enumerate) Fail(SME_ERR_INVALID_ARG, "enumeration runs in IN_MEMORY_GPU mode");
-    r = RunProgramExternal(prog, g->g, ctx, rb, re, o.ext_variant, 0);
+    r = RunProgramExternal(prog, g->g, ctx, rb, re, o.ext_variant, 0, o.root_stride);
     h2d = r.stats.h2d_bytes;
   } else {
     DeviceGraph* dg = g->g.dev;
@@ -105,7 +105,7 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
           Fail(SME_ERR_OOM, "cannot allocate enumeration buffer");
         }
       }
-      r = RunProgram(prog, *dg, ctx, rb, re, d_out, cap, o.warp_granularity);
+      r = RunProgram(prog, *dg, ctx, rb, re, d_out, cap, Tuning(o), o.root_stride);
       if (enumerate && cap && host_out) {
         uint64_t ncopy = std::min<uint64_t>(r.emitted, cap);
         if (ncopy) {

@@ -36,9 +36,9 @@ using namespace dev;
 // ---------------------------------------------------------------- kernels --
 namespace {
 
-__global__ void k_iota(uint32_t* out, uint32_t n, uint32_t start) {
+__global__ void k_iota(uint32_t* out, uint32_t n, uint32_t start, uint32_t stride) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = start + i;
+    out[i] = start + i * stride;
 }
 
 // Children estimate of an intersection step: the smallest list (the pivot
@@ -200,9 +200,10 @@ __global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __res
 // into a partner set), MODE 2 stores only the per-path count.
 template <int MODE>
 __global__ void __launch_bounds__(WARP_BLOCK) k_compute(
-    DFront F, DStep s, const uintE* __restrict__ rp, const uint32_t* __restrict__ cols,
-    const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr, uint32_t* out_cnt,
-    uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
+    DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
+    uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
+  const uintE* __restrict__ rp = G.rp;
+  const uint32_t* __restrict__ cols = G.cols;
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
@@ -212,15 +213,18 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute(
 
   for (uint32_t p = gw; p < F.P; p += nw) {
     const uint32_t* L[MAXV];
+    const uint32_t* B[MAXV];  // hub bitmap of the list (null: binary search)
     uint32_t N[MAXV];
     int nl = 0;
 #pragma unroll
     for (int i = 0; i < MAXV; ++i) {
+      B[i] = nullptr;
       if (i < s.nconn) {
         uint32_t v = F.inst[s.conn[i]][p];
         uintE b = rp[v], e = rp[v + 1];
         L[i] = cols + b;
         N[i] = (uint32_t)(e - b);
+        B[i] = HubBitmap(G, v);
         nl = i + 1;
       }
     }
@@ -244,6 +248,9 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute(
         const uint32_t* tp = L[0];
         L[0] = L[i];
         L[i] = tp;
+        tp = B[0];
+        B[0] = B[i];
+        B[i] = tp;
         uint32_t tn = N[0];
         N[0] = N[i];
         N[i] = tn;
@@ -290,9 +297,13 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute(
 #pragma unroll
       for (int j = 1; j < MAXV; ++j) {
         if (j < nl && ok) {
-          uint32_t pos = cur[j] + LowerBound(L[j] + cur[j], N[j] - cur[j], x);
-          cur[j] = pos;
-          ok = pos < N[j] && __ldg(L[j] + pos) == x;
+          if (B[j]) {
+            ok = BitTest(B[j], x);
+          } else {
+            uint32_t pos = cur[j] + LowerBound(L[j] + cur[j], N[j] - cur[j], x);
+            cur[j] = pos;
+            ok = pos < N[j] && __ldg(L[j] + pos) == x;
+          }
         }
       }
       unsigned mask = __ballot_sync(FULL, ok);
@@ -326,6 +337,206 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute(
     local = WarpSum(local);
     if (lane == 0 && local) atomicAdd(acc, local);
   }
+  if (lane == 0 && bytes) atomicAdd(acc + 1, bytes);
+}
+
+// ---- intersection, flattened over 32 paths per warp ------------------------
+// Same result as k_compute.  Each lane first prepares one path (lists, pivot,
+// clipped pivot range, excluded values) into shared memory; the warp then
+// walks the concatenation of the 32 pivot ranges 32 elements at a time, so
+// short pivots (the common case on skewed graphs) keep every lane busy.  A
+// lane finds its element's path by binary search over the 32 range offsets.
+// Sets stay sorted and compact per path: the rank of an element is its path's
+// running count plus the valid lanes before it in the same path segment.
+struct FlatPath {
+  const uint32_t* L[MAXV];  // L[0] = pivot (already offset by r0)
+  const uint32_t* B[MAXV];  // hub bitmaps (null: binary search)
+  uint32_t N[MAXV];
+  uint32_t ne[MAXV];
+  const uint32_t* W;        // ranked-count partner set
+  uint32_t WN;
+  uint64_t out_off;
+  uint32_t written;
+  uint8_t nl, nne;
+};
+constexpr int FLAT_WARPS = WARP_BLOCK / 32;
+
+template <int MODE>
+__global__ void __launch_bounds__(WARP_BLOCK) k_compute_flat(
+    DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
+    uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
+  const uintE* __restrict__ rp = G.rp;
+  const uint32_t* __restrict__ cols = G.cols;
+  __shared__ FlatPath sp[FLAT_WARPS][32];
+  __shared__ uint32_t soff[FLAT_WARPS][33];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long local = 0, bytes = 0;
+  const uint64_t base = (MODE == 0 && b0 > 0) ? est_incl[b0 - 1] : 0;
+  for (uint32_t p0 = gw * 32; p0 < F.P; p0 += nw * 32) {
+    const uint32_t p = p0 + lane;
+    uint32_t len = 0;
+    bool view = false;
+    if (p < F.P) {
+      FlatPath& fp = sp[wl][lane];
+      const uint32_t* L[MAXV];
+      const uint32_t* B[MAXV];
+      uint32_t N[MAXV];
+      int nl = 0;
+#pragma unroll
+      for (int i = 0; i < MAXV; ++i) {
+        B[i] = nullptr;
+        if (i < s.nconn) {
+          uint32_t v = F.inst[s.conn[i]][p];
+          uintE b = rp[v], e = rp[v + 1];
+          L[i] = cols + b;
+          N[i] = (uint32_t)(e - b);
+          B[i] = HubBitmap(G, v);
+          nl = i + 1;
+        }
+      }
+      if (s.reuse >= 0) {
+#pragma unroll
+        for (int i = 0; i < MAXV; ++i)
+          if (i == nl) GetSet(F, s.reuse, p, L[i], N[i]);
+        ++nl;
+      }
+      uint64_t b = 12ULL * s.nconn;
+#pragma unroll
+      for (int i = 0; i < MAXV; ++i)
+        if (i < nl) b += 4ULL * N[i];
+#pragma unroll
+      for (int i = 1; i < MAXV; ++i) {
+        if (i < nl && N[i] < N[0]) {
+          const uint32_t* tp = L[0];
+          L[0] = L[i];
+          L[i] = tp;
+          tp = B[0];
+          B[0] = B[i];
+          B[i] = tp;
+          uint32_t tn = N[0];
+          N[0] = N[i];
+          N[i] = tn;
+        }
+      }
+      Bounds bd = MakeBounds(s.cond, F, p);
+      uint32_t r0 = 0, r1 = 0;
+      if (nl > 0) Range(L[0], N[0], bd, r0, r1);
+      if (MODE == 0) {
+        fp.out_off = (p + b0 == 0 ? 0 : est_incl[p + b0 - 1]) - base;
+        if (nl == 1) {
+          uint32_t ex[MAXV];
+          if (Exclusions(L[0], r0, r1, bd, ex) == 0) {
+            out_ptr[p] = (uint64_t)(L[0] + r0);
+            out_cnt[p] = r1 - r0;
+            b += 4ULL * (r1 - r0);
+            view = true;
+          }
+        }
+      }
+      bytes += b;
+      fp.W = nullptr;
+      fp.WN = 0;
+      if (MODE == 1 && s.with_u >= 0) GetSet(F, s.with_u, p, fp.W, fp.WN);
+      fp.L[0] = L[0] + r0;
+      fp.N[0] = r1 - r0;
+#pragma unroll
+      for (int i = 1; i < MAXV; ++i) {
+        fp.L[i] = L[i];
+        fp.N[i] = N[i];
+        fp.B[i] = B[i];
+      }
+#pragma unroll
+      for (int i = 0; i < MAXV; ++i) fp.ne[i] = bd.ne[i];
+      fp.nne = (uint8_t)bd.nne;
+      fp.nl = (uint8_t)nl;
+      fp.written = 0;
+      len = view ? 0 : r1 - r0;
+    }
+    // exclusive scan of the pivot ranges of the 32 paths
+    uint32_t x = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(FULL, x, o);
+      if (lane >= o) x += y;
+    }
+    soff[wl][lane] = x - len;
+    const uint32_t total = __shfl_sync(FULL, x, 31);
+    if (lane == 31) soff[wl][32] = total;
+    __syncwarp();
+    for (uint32_t fb = 0; fb < total; fb += 32) {
+      const uint32_t f = fb + lane;
+      const bool in = f < total;
+      // path of element f: last j with soff[j] <= f
+      int j = 0;
+      if (in) {
+        int lo = 0, hi = 31;
+        while (lo < hi) {
+          int mid = (lo + hi + 1) >> 1;
+          if (soff[wl][mid] <= f) lo = mid;
+          else hi = mid - 1;
+        }
+        j = lo;
+      }
+      const FlatPath& fp = sp[wl][j];
+      bool ok = in;
+      uint32_t v = 0;
+      if (ok) {
+        v = __ldg(fp.L[0] + (f - soff[wl][j]));
+        for (int k = 0; k < fp.nne; ++k)
+          if (v == fp.ne[k]) ok = false;
+#pragma unroll
+        for (int q = 1; q < MAXV; ++q) {
+          if (q < fp.nl && ok) {
+            if (fp.B[q]) {
+              ok = BitTest(fp.B[q], v);
+            } else {
+              uint32_t pos = LowerBound(fp.L[q], fp.N[q], v);
+              ok = pos < fp.N[q] && __ldg(fp.L[q] + pos) == v;
+            }
+          }
+        }
+      }
+      const unsigned valid = __ballot_sync(FULL, ok);
+      if (MODE == 1) {
+        if (ok) local += fp.W ? RankCount(fp.W, fp.WN, v, s.with_op) : 1;
+      } else {
+        // segments of lanes that belong to the same path
+        const int jprev = __shfl_up_sync(FULL, j, 1);
+        const unsigned start = __ballot_sync(FULL, in && (lane == 0 || jprev != j));
+        const unsigned le = (lane == 31) ? FULL : ((2u << lane) - 1);
+        const int seg = 31 - __clz(start & le);
+        const unsigned segmask = (lane == 31 ? FULL : ((2u << lane) - 1)) & ~((1u << seg) - 1);
+        const uint32_t before = __popc(valid & segmask & ((1u << lane) - 1));
+        const uint32_t w0 = in ? sp[wl][j].written : 0;
+        if (MODE == 0 && ok) {
+          uint64_t o = fp.out_off + w0 + before;
+          if (o < out_cap) out_data[o] = v;
+          else atomicOr(err, ENGINE_ERR_BOUNDS);
+        }
+        __syncwarp();
+        // the last lane of each segment advances its path's running count
+        const int jnext = __shfl_down_sync(FULL, j, 1);
+        const bool last = in && (lane == 31 || f + 1 >= total || jnext != j);
+        if (last) sp[wl][j].written = w0 + before + (ok ? 1 : 0);
+        __syncwarp();
+      }
+      (void)valid;
+    }
+    if (MODE != 1 && p < F.P && !view) {  // views were published above
+      const FlatPath& fp = sp[wl][lane];
+      out_ptr[p] = MODE == 0 ? (uint64_t)(out_data + fp.out_off) : 0;
+      out_cnt[p] = fp.written;
+      if (MODE == 0) bytes += 4ULL * fp.written;
+    }
+    __syncwarp();
+  }
+  if (MODE == 1) {
+    local = WarpSum(local);
+    if (lane == 0 && local) atomicAdd(acc, local);
+  }
+  bytes = WarpSum(bytes);
   if (lane == 0 && bytes) atomicAdd(acc + 1, bytes);
 }
 
@@ -638,6 +849,57 @@ void DestroyContext(DeviceContext* c) {
   delete c;
 }
 
+namespace {
+__global__ void k_build_bitmaps(const uintE* __restrict__ rp, const uint32_t* __restrict__ cols,
+                                const uint32_t* __restrict__ hubs, uint32_t words, uint32_t* bm) {
+  const uint32_t v = hubs[blockIdx.x];
+  uint32_t* row = bm + (size_t)blockIdx.x * words;
+  for (uintE j = rp[v] + threadIdx.x; j < rp[v + 1]; j += blockDim.x) {
+    uint32_t w = cols[j];
+    atomicOr(row + (w >> 5), 1u << (w & 31));
+  }
+}
+
+// Bitmaps for the vertices of highest degree (>= kHubMinDegree) within a
+// byte budget (SME_HUB_BITMAP_MB, default 256 MiB); a bitmap is n bits.
+void BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream) {
+  const uint64_t kHubMinDegree = 256;
+  uint64_t budget = 256ULL << 20;
+  if (const char* e = std::getenv("SME_HUB_BITMAP_MB")) budget = std::strtoull(e, nullptr, 10) << 20;
+  const uint32_t words = (uint32_t)((g.n + 31) / 32);
+  if (budget == 0 || words == 0) return;
+  const uint64_t max_hubs = budget / ((uint64_t)words * 4);
+  std::vector<std::pair<uint64_t, uint32_t>> cand;
+  for (uint64_t u = 0; u < g.n; ++u) {
+    uint64_t deg = g.row_ptrs[u + 1] - g.row_ptrs[u];
+    if (deg >= kHubMinDegree) cand.emplace_back(deg, (uint32_t)u);
+  }
+  if (cand.empty() || max_hubs == 0) return;
+  std::sort(cand.begin(), cand.end(), [](const std::pair<uint64_t, uint32_t>& a,
+                                         const std::pair<uint64_t, uint32_t>& b) { return a.first > b.first; });
+  if (cand.size() > max_hubs) cand.resize(max_hubs);
+  std::vector<int32_t> slot(g.n, -1);
+  std::vector<uint32_t> hubs(cand.size());
+  for (size_t i = 0; i < cand.size(); ++i) {
+    hubs[i] = cand[i].second;
+    slot[cand[i].second] = (int32_t)i;
+  }
+  uint32_t* d_hubs = nullptr;
+  CK(cudaMalloc((void**)&d->hub_slot, g.n * sizeof(int32_t)));
+  CK(cudaMalloc((void**)&d->bitmaps, hubs.size() * (size_t)words * 4));
+  CK(cudaMalloc((void**)&d_hubs, hubs.size() * 4));
+  CK(cudaMemcpyAsync(d->hub_slot, slot.data(), g.n * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_hubs, hubs.data(), hubs.size() * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemsetAsync(d->bitmaps, 0, hubs.size() * (size_t)words * 4, stream));
+  k_build_bitmaps<<<(unsigned)hubs.size(), 256, 0, stream>>>(d->row_ptrs, d->cols, d_hubs, words, d->bitmaps);
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaGetLastError());
+  cudaFree(d_hubs);
+  d->words = words;
+  d->nhubs = (uint32_t)hubs.size();
+}
+}  // namespace
+
 DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, uint64_t* h2d) {
   CK(cudaSetDevice(device));
   auto* d = new DeviceGraph();
@@ -650,6 +912,7 @@ DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, ui
     CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, stream));
     if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
+    BuildHubBitmaps(d, g, stream);
   } catch (...) {
     FreeDeviceGraph(d);
     throw;
@@ -661,12 +924,10 @@ DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, ui
 void FreeDeviceGraph(DeviceGraph* d) {
   if (!d) return;
   cudaSetDevice(d->device);
-  if (d->host_mapped) {
-    if (d->row_ptrs) cudaFree(d->row_ptrs);
-  } else {
-    if (d->row_ptrs) cudaFree(d->row_ptrs);
-    if (d->cols) cudaFree(d->cols);
-  }
+  if (d->row_ptrs) cudaFree(d->row_ptrs);
+  if (d->cols && !d->host_mapped) cudaFree(d->cols);
+  if (d->hub_slot) cudaFree(d->hub_slot);
+  if (d->bitmaps) cudaFree(d->bitmaps);
   delete d;
 }
 
@@ -719,7 +980,8 @@ class Executor {
   uint64_t ext_h2d_bytes() const { return ext_bytes_; }
   uint64_t ext_loads() const { return ext_loads_; }
 
-  RunResult Run(uint64_t rb, uint64_t re) {
+  RunResult Run(uint64_t rb, uint64_t re, uint32_t stride = 1) {
+    if (stride == 0) stride = 1;
     auto t0 = std::chrono::steady_clock::now();
     size_t mark = A_.Mark();
     ctrl_ = (unsigned long long*)A_.Alloc(8 * sizeof(unsigned long long));
@@ -734,11 +996,13 @@ class Executor {
     const uint64_t per_root = 4 + 8 + 8;
     uint64_t chunk = std::max<uint64_t>(1, Budget(0) / per_root);
     chunk = std::min<uint64_t>(chunk, 0x7fffffffULL);
-    for (uint64_t b = rb; b < re; b += chunk) {
-      uint32_t P = (uint32_t)std::min<uint64_t>(chunk, re - b);
+    // roots rb, rb+stride, ... < re in chunks of `chunk` roots
+    const uint64_t nroots = R == 0 ? 0 : (R + stride - 1) / stride;
+    for (uint64_t i0 = 0; i0 < nroots; i0 += chunk) {
+      uint32_t P = (uint32_t)std::min<uint64_t>(chunk, nroots - i0);
       size_t m = A_.Mark();
       uint32_t* col = (uint32_t*)A_.Alloc((size_t)P * 4);
-      k_iota<<<Grid(P, 256), 256, 0, st_>>>(col, P, (uint32_t)b);
+      k_iota<<<Grid(P, 256), 256, 0, st_>>>(col, P, (uint32_t)(rb + i0 * stride), stride);
       Launched();
       DFront F{};
       F.P = P;
@@ -798,16 +1062,17 @@ class Executor {
   const uint32_t* ext_cols_ = nullptr;
   uint64_t ext_bytes_ = 0, ext_loads_ = 0;
 
-  struct GraphView {
-    const uintE* rp;
-    const uint32_t* cols;
-  };
-
   // Loads, for the paths of Fb, the adjacency lists step `ds` intersects into
   // a device subgraph allocated in the current arena frame (it stays valid
   // while deeper levels use candidate sets that point into it).
-  GraphView LoadSubgraph(const DFront& Fb, const DStep& ds) {
-    if (!ext_cols_) return GraphView{g_.row_ptrs, g_.cols};
+  // The resident graph with its hub bitmaps (`use_bitmaps_` false: lists only).
+  DGraph Resident() const {
+    if (use_bitmaps_ && g_.hub_slot) return DGraph{g_.row_ptrs, g_.cols, g_.hub_slot, g_.bitmaps, g_.words};
+    return DGraph{g_.row_ptrs, g_.cols, nullptr, nullptr, 0};
+  }
+
+  DGraph LoadSubgraph(const DFront& Fb, const DStep& ds) {
+    if (!ext_cols_) return Resident();
     const uint32_t n = (uint32_t)g_.n;
     const size_t mark = A_.Mark();
     uint8_t* flag = (uint8_t*)A_.Alloc(n);
@@ -838,7 +1103,7 @@ class Executor {
     ext_bytes_ += sub_m * 4;
     ++ext_loads_;
     (void)mark;
-    return GraphView{sub_rp, sub_cols};
+    return DGraph{sub_rp, sub_cols, nullptr, nullptr, 0};
   }
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events_;
 
@@ -849,6 +1114,29 @@ class Executor {
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)sms_ * 16));
   }
   unsigned WarpGrid(uint64_t paths) const { return Grid(paths * 32, WARP_BLOCK); }
+
+  // Intersection launch: warp per path (granularity 1) or flattened over 32
+  // paths per warp (default).
+  template <int MODE>
+  void Compute(const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est, uint32_t b0, uint64_t* ptr,
+               uint32_t* cnt, uint32_t* data, uint64_t cap) {
+    unsigned long long* acc = ctrl_;
+    uint32_t* err = (uint32_t*)(ctrl_ + 3);
+    auto t = TimerStart();
+    if (gran_ == 1)
+      k_compute<MODE><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+    else
+      k_compute_flat<MODE><<<WarpGrid((F.P + 31) / 32), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data,
+                                                                              cap, acc, err);
+    TimerStop(t);
+    Launched();
+  }
+
+ public:
+  int gran_ = 0;
+  bool use_bitmaps_ = true;
+
+ private:
 
   uint64_t Budget(size_t k) const {
     size_t rem = prog_.steps.size() - k + 1;
@@ -953,11 +1241,7 @@ class Executor {
       case S_COMPUTE_COUNT: {
         paths_ += F.P;
         if (!ext_cols_) {
-          auto t = TimerStart();
-          k_compute<1><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, g_.row_ptrs, g_.cols, nullptr, 0,
-                                                              nullptr, nullptr, nullptr, 0, acc, err);
-          TimerStop(t);
-          Launched();
+          Compute<1>(F, ds, Resident(), nullptr, 0, nullptr, nullptr, nullptr, 0);
           return;
         }
         // external: batches whose required lists fit the level budget
@@ -972,12 +1256,8 @@ class Executor {
           const size_t mk = A_.Mark();
           DFront Fb = Slice(F, b.b0, b.b1);
           ++batches_;
-          GraphView gv = LoadSubgraph(Fb, ds);
-          auto t = TimerStart();
-          k_compute<1><<<WarpGrid(Fb.P), WARP_BLOCK, 0, st_>>>(Fb, ds, gv.rp, gv.cols, nullptr, 0, nullptr,
-                                                               nullptr, nullptr, 0, acc, err);
-          TimerStop(t);
-          Launched();
+          DGraph gv = LoadSubgraph(Fb, ds);
+          Compute<1>(Fb, ds, gv, nullptr, 0, nullptr, nullptr, nullptr, 0);
           A_.Release(mk);
         }
         A_.Release(m0);
@@ -1039,16 +1319,11 @@ class Executor {
           uint32_t* cnt = (uint32_t*)A_.Alloc((size_t)Pb * 4);
           uint64_t cap = s.kind == S_COMPUTE ? b.e1 - b.e0 : 0;
           uint32_t* data = cap ? (uint32_t*)A_.Alloc(cap * 4) : nullptr;
-          GraphView gv = LoadSubgraph(Fb, ds);
-          auto t = TimerStart();
+          DGraph gv = LoadSubgraph(Fb, ds);
           if (s.kind == S_COMPUTE)
-            k_compute<0><<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, ds, gv.rp, gv.cols, est, b.b0, ptr,
-                                                               cnt, data, cap, acc, err);
+            Compute<0>(Fb, ds, gv, est, b.b0, ptr, cnt, data, cap);
           else
-            k_compute<2><<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, ds, gv.rp, gv.cols, est, b.b0, ptr,
-                                                               cnt, nullptr, 0, acc, err);
-          TimerStop(t);
-          Launched();
+            Compute<2>(Fb, ds, gv, est, b.b0, ptr, cnt, nullptr, 0);
           DFront Fn = Fb;
           Fn.set[s.u] = DSet{ptr, cnt};
           Fn.cidx[s.u] = nullptr;
@@ -1119,13 +1394,14 @@ class Executor {
 }  // namespace
 
 RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx, uint64_t rb,
-                     uint64_t re, uint32_t* d_out, uint64_t cap, int warp_granularity) {
-  (void)warp_granularity;
+                     uint64_t re, uint32_t* d_out, uint64_t cap, int tuning, uint32_t stride) {
   CK(cudaSetDevice(ctx.device));
   if (re > g.n) re = g.n;
   if (rb > re) rb = re;
   Executor ex(prog, g, ctx, d_out, cap);
-  return ex.Run(rb, re);
+  ex.gran_ = tuning & 0xff;
+  ex.use_bitmaps_ = !(tuning & 0x100);
+  return ex.Run(rb, re, stride);
 }
 
 // EXTERNAL_GPU: the graph stays in host memory.
@@ -1137,7 +1413,7 @@ RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& c
 //   EXT_UMA    the adjacency lists live in managed memory and migrate on
 //              demand (EXTUMALIGHTGPUComp, src/gpu/impl/light/ext/uma/).
 RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceContext& ctx, uint64_t rb,
-                             uint64_t re, int ext_variant, uint64_t graph_budget_bytes) {
+                             uint64_t re, int ext_variant, uint64_t graph_budget_bytes, uint32_t stride) {
   (void)graph_budget_bytes;
   CK(cudaSetDevice(ctx.device));
   if (re > hg.n) re = hg.n;
@@ -1158,7 +1434,7 @@ RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceCon
       if (hg.m) std::memcpy(managed, hg.cols, hg.m * sizeof(uintV));
       dg.cols = managed;
       Executor ex(prog, dg, ctx, nullptr, 0);
-      r = ex.Run(rb, re);
+      r = ex.Run(rb, re, stride);
       h2d += hg.m * sizeof(uintV);
     } else {
       const uint32_t* dcols = nullptr;
@@ -1175,7 +1451,7 @@ RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceCon
       }
       Executor ex(prog, dg, ctx, nullptr, 0);
       ex.SetExternal(dcols);
-      r = ex.Run(rb, re);
+      r = ex.Run(rb, re, stride);
       h2d += ex.ext_h2d_bytes();
     }
   } catch (...) {

@@ -14,6 +14,10 @@ struct DeviceGraph {
   uintE* row_ptrs = nullptr;
   uintV* cols = nullptr;
   bool host_mapped = false;  // cols live in mapped pinned host memory (EXT_UMA)
+  // dense adjacency bitmaps of the highest-degree vertices
+  int32_t* hub_slot = nullptr;  // per vertex: bitmap slot or -1
+  uint32_t* bitmaps = nullptr;  // nhubs x words
+  uint32_t words = 0, nhubs = 0;
 };
 
 // Stack allocator over one device allocation.  Levels are processed depth
@@ -55,12 +59,15 @@ struct RunResult {
 // prog.enumerate, instances are written to out (device) up to cap.
 RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx,
                      uint64_t root_begin, uint64_t root_end, uint32_t* d_out, uint64_t cap,
-                     int warp_granularity);
+                     int tuning, uint32_t root_stride = 1);
+// `tuning`: low byte = intersection granularity (0 auto, 1 warp per path,
+// 2 flattened); bit 8 set = no hub bitmaps.
+inline int Tuning(const sme_opts& o) { return (o.warp_granularity & 0xff) | (o.list_only ? 0x100 : 0); }
 
 // External (chunked) execution over a graph that stays in host memory.
 RunResult RunProgramExternal(const Program& prog, const HostGraph& g, DeviceContext& ctx,
                              uint64_t root_begin, uint64_t root_end, int ext_variant,
-                             uint64_t graph_budget_bytes);
+                             uint64_t graph_budget_bytes, uint32_t root_stride = 1);
 
 int DeviceCount();
 

@@ -102,7 +102,7 @@ struct sme_server {
         uint64_t re = r.opts.root_end ? std::min<uint64_t>(r.opts.root_end, hg.n) : hg.n;
         RunResult rr;
         try {
-          rr = RunProgram(prog, *dg, *ctx, r.opts.root_begin, re, nullptr, 0, 0);
+          rr = RunProgram(prog, *dg, *ctx, r.opts.root_begin, re, nullptr, 0, Tuning(r.opts), r.opts.root_stride);
         } catch (...) {
           if (temp) FreeDeviceGraph(dg);
           throw;

@@ -56,6 +56,27 @@ struct DMatOut {
   uint8_t keep;
 };
 
+// Graph as seen by the intersection kernels.  Vertices of the highest degree
+// also have a dense adjacency bitmap (`words` uint32 per hub): membership in
+// their lists is one load instead of a binary search over a long list.
+struct DGraph {
+  const uint64_t* rp;
+  const uint32_t* cols;
+  const int32_t* hub;  // hub slot per vertex, -1 none; null: no bitmaps
+  const uint32_t* bm;
+  uint32_t words;
+};
+
+__device__ __forceinline__ const uint32_t* HubBitmap(const DGraph& g, uint32_t v) {
+  if (!g.hub) return nullptr;
+  int32_t s = __ldg(g.hub + v);
+  return s < 0 ? nullptr : g.bm + (size_t)s * g.words;
+}
+
+__device__ __forceinline__ bool BitTest(const uint32_t* bm, uint32_t x) {
+  return (__ldg(bm + (x >> 5)) >> (x & 31)) & 1u;
+}
+
 __device__ __forceinline__ uint32_t SetIndex(const DFront& F, int u, uint32_t p) {
   const uint32_t* c = F.cidx[u];
   return c ? c[p] : p + F.ident_off[u];

@@ -25,6 +25,10 @@ def lib():
                                   C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]
         L.oracle_query_size.restype = C.c_int
         L.oracle_query_size.argtypes = [C.c_int]
+        L.oracle_wcoj_sample.restype = C.c_uint64
+        L.oracle_wcoj_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_void_p,
+                                         C.c_uint64, C.c_int, C.c_double, C.POINTER(C.c_uint64),
+                                         C.POINTER(C.c_double)]
         L.oracle_wcoj_strided.restype = C.c_uint64
         L.oracle_wcoj_strided.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_uint64,
                                           C.c_uint64, C.c_int]
@@ -44,6 +48,19 @@ def count_strided(row_ptrs, cols, q, stride, offset=0, threads=0, ordering=True)
     cl = np.ascontiguousarray(cols, dtype=np.uint32)
     return int(lib().oracle_wcoj_strided(rp.ctypes.data, cl.ctypes.data if len(cl) else None, len(rp) - 1, q,
                                          int(ordering), stride, offset, threads))
+
+
+def count_sample(row_ptrs, cols, q, roots, budget_s, threads=0, ordering=True):
+    """Time-bounded sample: (instances of completed roots, completed roots,
+    seconds); roots cut short by the deadline are discarded."""
+    rp = np.ascontiguousarray(row_ptrs, dtype=np.uint64)
+    cl = np.ascontiguousarray(cols, dtype=np.uint32)
+    rt = np.ascontiguousarray(roots, dtype=np.uint32)
+    done, el = C.c_uint64(0), C.c_double(0)
+    inst = lib().oracle_wcoj_sample(rp.ctypes.data, cl.ctypes.data if len(cl) else None, len(rp) - 1, q,
+                                    int(ordering), rt.ctypes.data, len(rt), threads, budget_s, C.byref(done),
+                                    C.byref(el))
+    return int(inst), int(done.value), float(el.value)
 
 
 def enumerate_sorted(row_ptrs, cols, q, ordering=True) -> np.ndarray:

@@ -32,6 +32,21 @@ def test_counts_match_reference_on_golden_graphs(graphs, golden, algo):
             assert got == want, (name, q, algo, got, want)
 
 
+@pytest.mark.parametrize("gran", [1, 2])
+def test_intersection_granularities(graphs, golden, gran):
+    # 1: warp per path, 2: flattened over 32 paths per warp
+    for name in ("rmat_s12_ef8", "ba_n600_m4", "k12"):
+        for q, want in golden[name]["counts"].items():
+            if want > GPU_LIMIT:
+                continue
+            for algo in ALGOS:
+                assert graphs[name].count(int(q), algo, warp_granularity=gran) == want, (name, q, algo, gran)
+    rp, cl = O.read_bin(golden_graph_path("er_n64_d12"))
+    for q in (0, 3, 4):
+        got = O.sort_rows(graphs["er_n64_d12"].enumerate(q, sme.GPU_LIGHT, warp_granularity=gran))
+        assert np.array_equal(got, O.enumerate_sorted(rp, cl, q))
+
+
 @pytest.mark.parametrize("level", [0, 1, 2, 3])
 def test_light_compress_levels(graphs, golden, level):
     for name in ("rmat_s10_ef8", "ba_n600_m4", "k12"):
