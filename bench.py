@@ -48,7 +48,14 @@ def parse():
     ap.add_argument("--tasks", type=int, default=2, help="root-range tasks per query")
     ap.add_argument("--q1-stride", type=int, default=1024, help="4-cycle: roots per strided task = n/stride")
     ap.add_argument("--q1-tasks", type=int, default=3, help="4-cycle: strided tasks in the step cycle")
-    ap.add_argument("--root-end", type=int, default=0, help="restrict roots to [0, root_end) (profiling)")
+    ap.add_argument("--root-end", type=int, default=0, help="restrict roots to [root_begin, root_end) (profiling)")
+    ap.add_argument("--root-begin", type=int, default=0)
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched / served measurements")
+    ap.add_argument("--batch-graphs", type=int, default=4096)
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--task-roots", type=int, default=256, help="served: roots per request task")
+    ap.add_argument("--load", type=float, default=2.0, help="served arrival rate / plain throughput")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--granularity", type=int, default=0, help="0 auto, 1 warp per path, 2 flattened")
@@ -121,14 +128,130 @@ def work_items(args, n):
     1/q1_stride slice of the roots."""
     qs = [int(q) for q in args.queries.split(",")]
     end = args.root_end or n
+    beg = args.root_begin
     items = []
     for q in qs:
         if q == 1 and not args.root_end:
             items += [(q, k, end, args.q1_stride) for k in range(args.q1_tasks)]
         else:
-            cuts = [end * i // args.tasks for i in range(args.tasks + 1)]
+            cuts = [beg + (end - beg) * i // args.tasks for i in range(args.tasks + 1)]
             items += [(q, a, b, 1) for a, b in zip(cuts, cuts[1:])]
     return items
+
+
+def small_graph_batch(num, seed):
+    """The batched configuration: graphs log-uniform over 64..4096 vertices,
+    half Erdos-Renyi and half Barabasi-Albert, average degree U[4, 32];
+    queries uniform over triangle, 4-cycle, diamond, 4-clique."""
+    import random
+    import subgraphmatchgpu_b200 as sme
+    rnd = random.Random(seed)
+    gs, qs = [], []
+    for i in range(num):
+        n = int(round(2 ** rnd.uniform(6, 12)))
+        d = rnd.uniform(4, 32)
+        if i % 2 == 0:
+            gs.append(sme.Graph.er(n, d, seed=seed * 100003 + i))
+        else:
+            gs.append(sme.Graph.ba(n, max(1, int(round(d / 2))), seed=seed * 100003 + i))
+        qs.append(rnd.choice([0, 1, 2, 3]))
+    return gs, qs
+
+
+def bench_batched(args, device):
+    """Batched form vs the plain path (one sme_count per graph, graph copied
+    to the device per call) on the same small graphs."""
+    import numpy as np
+    import subgraphmatchgpu_b200 as sme
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as O
+    gs, qs = small_graph_batch(args.batch_graphs, 77)
+    t0 = time.perf_counter()
+    plan = sme.BatchPlan(gs, qs, autotune=True, use_graph=True, device=device)
+    prep_s = time.perf_counter() - t0
+    counts, _ = plan.run()
+    runs = []
+    for _ in range(3):
+        c, t = plan.run()
+        runs.append(t)
+        if not np.array_equal(c, counts):
+            raise RuntimeError("batched counts differ between replays")
+    ms = min(runs)
+    total = int(counts.sum())
+    t0 = time.perf_counter()
+    plain = [g.count(q, sme.GPU_LIGHT, device=device) for g, q in zip(gs, qs)]
+    plain_s = time.perf_counter() - t0
+    ok_plain = all(int(a) == int(b) for a, b in zip(plain, counts))
+    idx = list(range(0, len(gs), max(1, len(gs) // 64)))
+    ok_cpu = all(O.count(*gs[i].csr(), qs[i]) == int(counts[i]) for i in idx)
+    d = plan.describe()
+    plan.close()
+    return {"graphs": len(gs), "instances": total,
+            "batched": {"value": total / (ms / 1e3), "unit": UNIT, "ms": ms, "prepare_autotune_s": prep_s,
+                        "group_threads": d["group_threads"], "block_threads": d["block_threads"],
+                        "work_items": d["work_items"], "cuda_graph": True},
+            "plain": {"value": total / plain_s, "unit": UNIT, "ms": plain_s * 1e3},
+            "counts_equal_plain": ok_plain, "counts_equal_cpu_sample": ok_cpu, "cpu_checked_graphs": len(idx)}
+
+
+def bench_served(args, device):
+    """Served form: Poisson arrivals; each request is one pattern on a root
+    task of a resident R-MAT graph (s16/s18/s20, ef16) or on an attached
+    Erdos-Renyi graph (256..8192 vertices, degree 8).  Reports p50/p99 of
+    submit-to-result latency and instances/s, against the same requests run
+    one at a time through the plain path."""
+    import random
+    import numpy as np
+    import subgraphmatchgpu_b200 as sme
+    rnd = random.Random(5)
+    resident = [sme.Graph.rmat(s, 16, seed=100 + s) for s in (16, 18, 20)]
+    srv = sme.Server(slots=args.slots, device=device)
+    gids = [srv.add_graph(g) for g in resident]
+    pats = [0, 1, 2, 3, 4, 7]
+    reqs = []
+    for i in range(args.requests):
+        q = rnd.choice(pats)
+        if rnd.random() < 0.5:
+            n = rnd.randint(256, 8192)
+            reqs.append((q, -1, sme.Graph.er(n, 8.0, seed=9000 + i), 0, 0, 1))
+        else:
+            k = rnd.randrange(3)
+            n = resident[k].n
+            stride = max(1, n // args.task_roots)
+            off = rnd.randrange(stride)
+            reqs.append((q, gids[k], None, off, n, stride))
+    lat_plain, inst = [], 0
+    t0 = time.perf_counter()
+    for q, gid, att, a, b, st in reqs:
+        g = att if att is not None else resident[gid]
+        s0 = time.perf_counter()
+        inst += g.count(q, sme.GPU_LIGHT, root_begin=a, root_end=b, root_stride=st, device=device)
+        lat_plain.append((time.perf_counter() - s0) * 1e3)
+    plain_s = time.perf_counter() - t0
+    rate = args.load * len(reqs) / plain_s
+    ids, t_start = [], time.perf_counter()
+    t_next = t_start
+    for q, gid, att, a, b, st in reqs:
+        t_next += rnd.expovariate(rate)
+        while time.perf_counter() < t_next:
+            time.sleep(0.0002)
+        ids.append(srv.submit(q, gid=gid, attached=att, root_begin=a, root_end=b, root_stride=st))
+    res = [srv.wait(i) for i in ids]
+    served_s = time.perf_counter() - t_start
+    lat = [r[1] for r in res]
+    got = [r[0] for r in res]
+    alone = []
+    for q, gid, att, a, b, st in reqs[:16]:
+        alone.append(srv.wait(srv.submit(q, gid=gid, attached=att, root_begin=a, root_end=b, root_stride=st))[0])
+    stats = srv.stats()
+    srv.close()
+    inst_served = int(sum(got))
+    return {"requests": len(reqs), "arrival_rate_per_s": rate, "slots": args.slots,
+            "served": {"value": inst_served / served_s, "unit": UNIT, "p50_ms": float(np.percentile(lat, 50)),
+                       "p99_ms": float(np.percentile(lat, 99)), "max_inflight": stats["max_inflight"]},
+            "plain": {"value": inst / plain_s, "unit": UNIT, "p50_ms": float(np.percentile(lat_plain, 50)),
+                      "p99_ms": float(np.percentile(lat_plain, 99))},
+            "counts_equal_alone_and_in_mix": got[:16] == alone and inst_served == inst}
 
 
 def load_traffic():
@@ -248,9 +371,11 @@ def main():
         hot += s.hot_launches
         launches += s.kernel_launches
         q = items[(args.warmup + i) % len(items)][0]
-        per_query.setdefault(q, [0, 0.0])
+        per_query.setdefault(q, [0, 0.0, [0.0] * 8])
         per_query[q][0] += c
         per_query[q][1] += s.device_ms
+        for k in range(8):
+            per_query[q][2][k] += s.phase_ms[k]
     torch.cuda.synchronize()
     clk = clocks.stop()
     if dist:
@@ -300,6 +425,14 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, _, _ = cpu_baseline(g, items, args.cpu_seconds)
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = {}
+        for name, fn in (("batched", bench_batched), ("served", bench_served)):
+            try:
+                forms[name] = fn(args, local)
+            except Exception as e:  # reported in the line, never dropped silently
+                forms[name] = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         line = {
@@ -309,12 +442,15 @@ def main():
             "config": {"workload": f"R-MAT s{args.scale} ef{args.edge_factor} (a,b,c)=(.57,.19,.19) seed "
                                    f"{args.seed}: n={n} m={m} max_degree={dmax}; queries {args.queries} "
                                    f"(Q3 4-clique, Q1 4-cycle, Q2 diamond), plan algo {args.algo} "
-                                   f"(6=LIGHT), IN_MEMORY_GPU, {args.tasks} root tasks per query",
+                                   f"(6=LIGHT), IN_MEMORY_GPU; tasks: {args.tasks} root ranges per query, "
+                                   f"4-cycle {args.q1_tasks} strided tasks of every {args.q1_stride}-th root",
                        "l2": "inputs larger than L2 (CSR bytes %d)" % (8 * (n + 1) + 4 * m),
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "per_query": {str(q): {"instances": v[0], "device_ms": v[1]} for q, v in per_query.items()}},
+                       "per_query": {str(q): {"instances": v[0], "device_ms": v[1],
+                                              "phase_ms": dict(zip(sme.Stats.PHASES, [round(x, 3) for x in v[2]]))}
+                                     for q, v in per_query.items()}},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
-            "gpu_launches": launches,
+            "gpu_launches": launches, "forms": forms,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -100,6 +100,12 @@ typedef struct sme_stats {
   double device_ms;           /* CUDA-event time on the library's stream from
                                  the first to the last kernel of the run      */
   uint64_t hot_launches;      /* launches of the intersection kernels         */
+  /* CUDA-event time per phase (the reference's PROFILE phase timers,
+   * src/gpu/impl/common/ProfilerHelper.cuh:9-75): [0] compute,
+   * [1] materialize, [2] filter_compute, [3] compute_count,
+   * [4] compute_path_count, [5] count, [6] organize_batch (estimates, scans),
+   * [7] external subgraph load. */
+  double phase_ms[8];
 } sme_stats;
 
 /* ---- options ------------------------------------------------------------- */

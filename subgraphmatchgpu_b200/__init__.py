@@ -59,8 +59,14 @@ class Stats(C.Structure):
         ("elapsed_ms", C.c_double), ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64),
         ("batches", C.c_uint64), ("algorithmic_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64),
         ("d2h_bytes", C.c_uint64), ("peak_device_bytes", C.c_uint64), ("paths_processed", C.c_uint64),
-        ("device_ms", C.c_double), ("hot_launches", C.c_uint64),
+        ("device_ms", C.c_double), ("hot_launches", C.c_uint64), ("phase_ms", C.c_double * 8),
     ]
+
+    PHASES = ("compute", "materialize", "filter_compute", "compute_count", "compute_path_count", "count",
+              "organize_batch", "external_load")
+
+    def phases(self):
+        return {k: self.phase_ms[i] for i, k in enumerate(self.PHASES)}
 
 
 class BatchOpts(C.Structure):

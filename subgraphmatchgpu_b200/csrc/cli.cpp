@@ -117,7 +117,12 @@ int main(int argc, char** argv) {
   }
   sme_stats s;
   sme_last_stats(&s);
-  std::cout << "kernel_time=" << s.kernel_ms << "ms,batches=" << s.batches
+  static const char* kPhases[8] = {"compute_time",        "materialize_time",        "filter_compute_time",
+                                   "compute_count_time",  "compute_path_count_time", "count_time",
+                                   "organize_batch_time", "load_subgraph_time"};
+  for (int i = 0; i < 8; ++i)
+    if (s.phase_ms[i] > 0) std::cout << kPhases[i] << "=" << s.phase_ms[i] << "ms" << std::endl;
+  std::cout << "kernel_time=" << s.kernel_ms << "ms,device_time=" << s.device_ms << "ms,batches=" << s.batches
             << ",kernel_launches=" << s.kernel_launches << ",peak_device_bytes=" << s.peak_device_bytes
             << std::endl;
   std::cout << "total_match_count=" << count << ", elapsed_time=" << s.elapsed_ms << "ms" << std::endl;

@@ -33,6 +33,16 @@ using namespace dev;
     if (e_ != cudaSuccess) Fail(SME_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// sme_stats.phase_ms indices
+constexpr int kPhaseCompute = 0, kPhaseMaterialize = 1, kPhaseFilter = 2, kPhaseComputeCount = 3,
+              kPhasePathCount = 4, kPhaseCount = 5, kPhaseOrganize = 6, kPhaseExternal = 7;
+
+// A timed region on the execution stream (two CUDA events) and its phase.
+struct Timed {
+  cudaEvent_t a, b;
+  int phase;
+};
+
 // ---------------------------------------------------------------- kernels --
 namespace {
 
@@ -1030,16 +1040,18 @@ class Executor {
     r.stats.batches = batches_;
     r.stats.peak_device_bytes = A_.peak;
     r.stats.paths_processed = paths_;
-    float ms_total = 0;
+    double phase[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (auto& e : events_) {
       float ms = 0;
-      cudaEventElapsedTime(&ms, e.first, e.second);
-      ms_total += ms;
-      cudaEventDestroy(e.first);
-      cudaEventDestroy(e.second);
+      cudaEventElapsedTime(&ms, e.a, e.b);
+      phase[e.phase] += ms;
+      cudaEventDestroy(e.a);
+      cudaEventDestroy(e.b);
     }
     events_.clear();
-    r.stats.kernel_ms = ms_total;
+    for (int i = 0; i < 8; ++i) r.stats.phase_ms[i] = phase[i];
+    // the intersection kernels: COMPUTE, COMPUTE_COUNT, COMPUTE_PATH_COUNT
+    r.stats.kernel_ms = phase[kPhaseCompute] + phase[kPhaseComputeCount] + phase[kPhasePathCount];
     r.stats.device_ms = dev_ms;
     r.stats.hot_launches = hot_;
     r.stats.elapsed_ms =
@@ -1073,6 +1085,7 @@ class Executor {
 
   DGraph LoadSubgraph(const DFront& Fb, const DStep& ds) {
     if (!ext_cols_) return Resident();
+    Timed tl = TimerStart();
     const uint32_t n = (uint32_t)g_.n;
     const size_t mark = A_.Mark();
     uint8_t* flag = (uint8_t*)A_.Alloc(n);
@@ -1102,10 +1115,11 @@ class Executor {
     launches_ += 3;
     ext_bytes_ += sub_m * 4;
     ++ext_loads_;
+    TimerStop(tl, kPhaseExternal);
     (void)mark;
     return DGraph{sub_rp, sub_cols, nullptr, nullptr, 0};
   }
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events_;
+  std::vector<Timed> events_;
 
   void Launched() { ++launches_; }
 
@@ -1122,13 +1136,13 @@ class Executor {
                uint32_t* cnt, uint32_t* data, uint64_t cap) {
     unsigned long long* acc = ctrl_;
     uint32_t* err = (uint32_t*)(ctrl_ + 3);
-    auto t = TimerStart();
+    Timed t = TimerStart();
     if (gran_ == 1)
       k_compute<MODE><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
     else
       k_compute_flat<MODE><<<WarpGrid((F.P + 31) / 32), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data,
                                                                               cap, acc, err);
-    TimerStop(t);
+    TimerStop(t, MODE == 0 ? kPhaseCompute : MODE == 1 ? kPhaseComputeCount : kPhasePathCount);
     Launched();
   }
 
@@ -1143,17 +1157,20 @@ class Executor {
     return (uint64_t)((double)A_.Free() * 0.85 / (double)rem);
   }
 
-  std::pair<cudaEvent_t, cudaEvent_t> TimerStart() {
-    std::pair<cudaEvent_t, cudaEvent_t> e;
-    cudaEventCreate(&e.first);
-    cudaEventCreate(&e.second);
-    cudaEventRecord(e.first, st_);
+  Timed TimerStart() {
+    Timed e;
+    cudaEventCreate(&e.a);
+    cudaEventCreate(&e.b);
+    cudaEventRecord(e.a, st_);
+    e.phase = 0;
     return e;
   }
-  void TimerStop(std::pair<cudaEvent_t, cudaEvent_t> e) {
-    cudaEventRecord(e.second, st_);
+  // Records the end of a timed region of `phase` (sme_stats.phase_ms index).
+  void TimerStop(Timed e, int phase) {
+    cudaEventRecord(e.b, st_);
+    e.phase = phase;
     events_.push_back(e);
-    ++hot_;
+    if (phase == kPhaseCompute || phase == kPhaseComputeCount || phase == kPhasePathCount) ++hot_;
   }
 
   void Scan(uint64_t* d, uint32_t n) {
@@ -1264,6 +1281,7 @@ class Executor {
         return;
       }
       case S_COUNT: {
+        Timed tc = TimerStart();
         if (s.direct) {
           uint8_t us[3] = {0, 0, 0};
           for (size_t i = 0; i < s.unmat.size() && i < 3; ++i) us[i] = s.unmat[i];
@@ -1274,6 +1292,7 @@ class Executor {
         } else {
           k_count2<<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, s.unmat[0], s.unmat[1], s.pair_op, acc);
         }
+        TimerStop(tc, kPhaseCount);
         Launched();
         return;
       }
@@ -1284,6 +1303,7 @@ class Executor {
     uint64_t* est = (uint64_t*)A_.Alloc((size_t)F.P * 8);
     uint64_t* sumdeg = nullptr;  // external mode: subgraph bytes per path
     double pf = 0, cf = 0;
+    Timed to = TimerStart();
     if (s.kind == S_COMPUTE || s.kind == S_PATH_COUNT) {
       if (ext_cols_) sumdeg = (uint64_t*)A_.Alloc((size_t)F.P * 8);
       k_est_compute<<<Grid(F.P, 256), 256, 0, st_>>>(F, ds, g_.row_ptrs, est, sumdeg);
@@ -1302,6 +1322,7 @@ class Executor {
     Launched();
     Scan(est, F.P);
     if (sumdeg) Scan(sumdeg, F.P);
+    TimerStop(to, kPhaseOrganize);
     uint64_t budget = Budget(k);
     // keep child counts of a batch within 31-bit path indices
     budget = std::min<uint64_t>(budget, (uint64_t)(std::max(cf, 1.0) * 2.0e9));
@@ -1336,8 +1357,10 @@ class Executor {
           uint32_t* cnt = (uint32_t*)A_.Alloc((size_t)Pb * 4);
           uint64_t cap = b.e1 - b.e0;
           uint32_t* data = cap ? (uint32_t*)A_.Alloc(cap * 4) : nullptr;
+          Timed tf = TimerStart();
           k_filter<<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, s.u, ToDCond(s.cond), est, b.b0, ptr, cnt, data,
                                                          cap, err);
+          TimerStop(tf, kPhaseFilter);
           Launched();
           DFront Fn = Fb;
           Fn.set[s.u] = DSet{ptr, cnt};
@@ -1349,6 +1372,7 @@ class Executor {
         case S_MATERIALIZE: {
           DCond dc = ToDCond(s.cond);
           uint64_t* cnt = (uint64_t*)A_.Alloc((size_t)Pb * 8);
+          Timed tm = TimerStart();
           k_mat_count<<<Grid(Pb, 256), 256, 0, st_>>>(Fb, s.u, dc, cnt);
           Launched();
           Scan(cnt, Pb);
@@ -1368,9 +1392,8 @@ class Executor {
             o.sets[i] = s.sets_after[i];
             o.cidx[s.sets_after[i]] = (uint32_t*)A_.Alloc(C * 4);
           }
-          auto t = TimerStart();
           k_mat_write<<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, dc, o, cnt, C, err);
-          TimerStop(t);
+          TimerStop(tm, kPhaseMaterialize);
           Launched();
           DFront Fn{};
           Fn.P = (uint32_t)C;
