@@ -78,14 +78,14 @@ def test_batched_form_all_queries():
 
 
 def test_served_form_results_same_alone_and_in_mix():
-    big = sme.Graph.rmat(14, 16, seed=3)
-    mid = sme.Graph.rmat(12, 16, seed=4)
+    big = sme.Graph.rmat(12, 8, seed=3)
+    mid = sme.Graph.rmat(10, 8, seed=4)
     srv = sme.Server(slots=4)
     gids = [srv.add_graph(big), srv.add_graph(mid)]
     attached = [sme.Graph.er(n, 8.0, seed=n) for n in (256, 1024, 4096)]
     reqs = []
     rnd = random.Random(1)
-    for i in range(40):
+    for i in range(30):
         q = rnd.choice([0, 1, 2, 3, 4, 7])
         if i % 3 == 2:
             reqs.append((q, -1, attached[i % 3]))
