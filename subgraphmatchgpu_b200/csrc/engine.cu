@@ -207,9 +207,11 @@ __global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __res
 // in the other lists by a per-lane binary search whose lower end advances with
 // the lane's previous hit (each lane sees increasing candidates).
 // MODE 0 writes the sorted candidate set, MODE 1 counts (optionally ranked
-// into a partner set), MODE 2 stores only the per-path count.
-template <int MODE>
-__global__ void __launch_bounds__(WARP_BLOCK) k_compute(
+// into a partner set), MODE 2 stores only the per-path count.  MINB is the
+// minimum resident blocks per SM asked of the register allocator (the
+// kernels are latency bound: more resident warps, more searches in flight).
+template <int MODE, int MINB = 1>
+__global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
     uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
   const uintE* __restrict__ rp = G.rp;
@@ -1137,8 +1139,15 @@ class Executor {
     unsigned long long* acc = ctrl_;
     uint32_t* err = (uint32_t*)(ctrl_ + 3);
     Timed t = TimerStart();
-    if (gran_ == 1)
+    // granularity 0 (auto): steps that intersect a cached set (short pivots)
+    // use the flattened kernel, the others warp per path
+    int gran = gran_ ? gran_ : (ds.reuse >= 0 ? 2 : 3);
+    if (gran == 1)
       k_compute<MODE><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+    else if (gran == 3)
+      k_compute<MODE, 4><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+    else if (gran == 4)
+      k_compute<MODE, 6><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
     else
       k_compute_flat<MODE><<<WarpGrid((F.P + 31) / 32), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data,
                                                                               cap, acc, err);

@@ -5,8 +5,10 @@
 // runs one request at a time through the level engine; requests of different
 // patterns and graphs therefore run concurrently on the device.  A request is
 // admitted when a slot is idle and the sum of the estimated frontier bytes of
-// the requests in flight stays within the server budget; otherwise it waits
-// in the FIFO queue (the head is never overtaken, so no request starves).
+// the requests in flight stays within the server budget.  Among the queued
+// requests that fit, the one with the least estimated work goes first, so
+// short requests are not stuck behind long ones; a request that has waited
+// longer than kStarveMs goes first regardless (nothing starves).
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -31,8 +33,24 @@ struct Request {
   sme_graph* attached;
   sme_opts opts;
   uint64_t est_bytes;
+  double est_work;
   Clock::time_point submitted;
 };
+
+constexpr double kStarveMs = 500.0;
+
+// Work estimate used only to order admission: roots of the task times the
+// average degree to the power of the pattern's later levels.
+double EstimateWork(const HostGraph& g, const sme_opts& o) {
+  const int k = Query(o.query_type).n;
+  const uint64_t end = o.root_end ? std::min<uint64_t>(o.root_end, g.n) : g.n;
+  const uint64_t stride = o.root_stride ? o.root_stride : 1;
+  const double roots = end > o.root_begin ? (double)((end - o.root_begin + stride - 1) / stride) : 0.0;
+  const double davg = g.n ? (double)g.m / (double)g.n : 0.0;
+  double w = roots;
+  for (int i = 1; i < k; ++i) w *= std::max(1.0, davg);
+  return w;
+}
 
 struct Result {
   sme_status status = SME_ERR_BUSY;
@@ -71,6 +89,20 @@ struct sme_server {
   bool stop = false;
   uint64_t slot_arena = 0;
 
+  // Index of the queued request to admit next, or -1 (caller holds mu).
+  long Pick() const {
+    if (queue.empty()) return -1;
+    auto fits = [&](const Request& r) { return inflight == 0 || inflight_bytes + r.est_bytes <= o.mem_budget_bytes; };
+    const double age =
+        std::chrono::duration<double, std::milli>(Clock::now() - queue.front().submitted).count();
+    if (age > kStarveMs) return fits(queue.front()) ? 0 : -1;
+    long best = -1;
+    const size_t scan = std::min<size_t>(queue.size(), 256);
+    for (size_t i = 0; i < scan; ++i)
+      if (fits(queue[i]) && (best < 0 || queue[i].est_work < queue[best].est_work)) best = (long)i;
+    return best;
+  }
+
   void Worker(int slot) {
     cudaSetDevice(o.device);
     DeviceContext* ctx = ctxs[slot];
@@ -78,13 +110,16 @@ struct sme_server {
       Request r;
       {
         std::unique_lock<std::mutex> l(mu);
-        cv_work.wait(l, [&] {
-          return stop || (!queue.empty() && (inflight == 0 || inflight_bytes + queue.front().est_bytes <=
-                                                                   o.mem_budget_bytes));
-        });
-        if (stop && queue.empty()) return;
-        r = queue.front();
-        queue.pop_front();
+        long pick = -1;
+        // wake at least every kStarveMs so ageing is noticed without new work
+        while (!(stop && queue.empty())) {
+          pick = Pick();
+          if (pick >= 0) break;
+          cv_work.wait_for(l, std::chrono::milliseconds((long)kStarveMs));
+        }
+        if (pick < 0) return;  // stopping and the queue is empty
+        r = queue[pick];
+        queue.erase(queue.begin() + pick);
         inflight_bytes += r.est_bytes;
         ++inflight;
         max_inflight = std::max(max_inflight, inflight);
@@ -215,6 +250,7 @@ sme_status sme_server_submit(sme_server* s, int32_t gid, sme_graph* attached, co
       const HostGraph& hg = attached ? attached->g : s->resident[gid]->g;
       Compile(r.opts, false);  // validate query / plan before queueing
       r.est_bytes = EstimateBytes(hg, r.opts.query_type);
+      r.est_work = EstimateWork(hg, r.opts);
       r.id = s->next_id++;
       s->results[r.id] = Result();
       s->queue.push_back(r);
