@@ -277,6 +277,19 @@ def bench_served(args, device):
             "counts_equal_alone_and_in_mix": same}
 
 
+def reduce_over_ranks(dev_ms, instances, dist, device):
+    """Replicas: the job's time is the slowest rank's device time, its work
+    the sum of the ranks' instances (timing only; no data-path collective)."""
+    if dist is None:
+        return dev_ms, float(instances)
+    import torch
+    tmax = torch.tensor([float(dev_ms)], dtype=torch.float64, device=device)
+    tsum = torch.tensor([float(instances)], dtype=torch.float64, device=device)
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax.item()), float(tsum.item())
+
+
 def load_traffic():
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
@@ -401,14 +414,7 @@ def main():
             per_query[q][2][k] += s.phase_ms[k]
     torch.cuda.synchronize()
     clk = clocks.stop()
-    if dist:
-        t = torch.tensor([dev_ms, total_inst], dtype=torch.float64, device="cuda")
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        dev_ms_max, inst_all = float(tmax[0]), float(t[1])
-    else:
-        dev_ms_max, inst_all = dev_ms, float(total_inst)
+    dev_ms_max, inst_all = reduce_over_ranks(dev_ms, total_inst, dist, "cuda")
     value = inst_all / (dev_ms_max / 1e3)
 
     # end to end through the C-ABI: CSR in pinned host memory, copied every step

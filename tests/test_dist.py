@@ -1,0 +1,52 @@
+"""The N>1 bench path (replicas) on CPU: two gloo ranks reduce their device
+times (max) and instance counts (sum) the way bench.py does on NCCL."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    import bench
+    t, inst = bench.reduce_over_ranks(100.0 + 50.0 * rank, 1000 * (rank + 1), dist, "cpu")
+    q.put((rank, t, inst))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_reduction_two_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, t, inst in res:
+        assert t == 150.0 and inst == 3000.0
+
+
+def test_single_process_is_identity():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.reduce_over_ranks(12.5, 7, None, "cpu") == (12.5, 7.0)
