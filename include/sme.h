@@ -201,6 +201,24 @@ sme_status sme_batch_describe(const sme_batch_plan* p, int32_t* granularity,
                               int32_t* block_threads, uint64_t* work_items);
 sme_status sme_batch_free(sme_batch_plan* p);
 
+/* Allocation-free count of query `query_type` on one graph whose CSR the
+ * caller already holds in device memory (d_row_ptrs: n+1 uint64 offsets,
+ * d_cols: uint32 neighbour ids, sorted lists, both directions stored).  It has
+ * no counterpart in the reference.  It exists for callers that must not call
+ * cudaMalloc: code running under a framework whose caching allocator already
+ * owns the device memory, or latency-critical paths that cannot afford an
+ * allocation and the synchronisation it implies.  Besides the caller's
+ * buffers it uses only a 16 MiB array the library reserves in device memory
+ * for the life of the process on every GPU that loads it; nothing is
+ * allocated or freed.  Limit: the graph's maximum degree must be at most
+ * 32768 and n below 2^31, else SME_ERR_CAPACITY / SME_ERR_INVALID_ARG.
+ * The first call on a device looks up the array's device address, so make
+ * that first call before any stream capture.  Calls run on the legacy default
+ * stream and return when the count is known; all calls share the one array,
+ * so calls that overlap on the same GPU (from several host threads) race. */
+sme_status sme_count_noalloc(const uint64_t* d_row_ptrs, const uint32_t* d_cols,
+                             uint64_t n, int32_t query_type, uint64_t* count);
+
 /* ---- served form: resident graphs + continuous batching ----------------- */
 typedef struct sme_server sme_server;
 typedef struct sme_server_opts {

@@ -117,6 +117,7 @@ SIGNATURES = {
     "sme_batch_run": (C.c_int, [_P, _P, C.POINTER(C.c_double)]),
     "sme_batch_describe": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _PU64]),
     "sme_batch_free": (C.c_int, [_P]),
+    "sme_count_noalloc": (C.c_int, [_P, _P, _U64, C.c_int32, _PU64]),
     "sme_server_opts_default": (C.c_int, [C.POINTER(ServerOpts)]),
     "sme_server_create": (C.c_int, [C.POINTER(ServerOpts), _PP]),
     "sme_server_add_graph": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <chrono>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "engine.h"
@@ -94,8 +95,8 @@ struct Tile {
 // Candidate set of level `l` for the current partial instance M: written to
 // `out` (when non-null) or counted.  Returns the group-uniform size; when the
 // set is a single clipped list without exclusions, *view points into it.
-template <int G>
-__device__ uint32_t LevelSet(const Tile<G>& t, const BLevel& L, const uint32_t* M, const uint32_t* rp,
+template <int G, typename RP>
+__device__ uint32_t LevelSet(const Tile<G>& t, const BLevel& L, const uint32_t* M, const RP* rp,
                              const uint32_t* cols, const uint32_t* const* sptr, const uint32_t* slen,
                              uint32_t* out, const uint32_t** view, bool pair_count,
                              unsigned long long* cnt) {
@@ -107,7 +108,7 @@ __device__ uint32_t LevelSet(const Tile<G>& t, const BLevel& L, const uint32_t* 
     if (i < L.nconn) {
       uint32_t v = M[L.conn[i]];
       A[i] = cols + rp[v];
-      N[i] = rp[v + 1] - rp[v];
+      N[i] = (uint32_t)(rp[v + 1] - rp[v]);
       nl = i + 1;
     }
   }
@@ -323,6 +324,134 @@ int MaxBuffers(const std::vector<int32_t>& queries) {
     nb = std::max(nb, c);
   }
   return std::max(nb, 1);
+}
+
+// ---- allocation-free single-graph count (sme_count_noalloc) ---------------
+// Library-owned device memory, reserved when the library is loaded and kept
+// by every GPU that loads it until the process exits: 16 MiB.  Words [0,64)
+// hold one call's control values (word 0: next work item, words 2-3: the
+// uint64 count, word 4: the graph's maximum degree); the rest holds the
+// thread groups' level buffers.  Every call reuses (and first clears) it.
+constexpr size_t kNoAllocWords = size_t(4) << 20;
+constexpr size_t kNoAllocHeader = 64;
+constexpr uint32_t kNoAllocMaxDegree = 32768;
+constexpr int kNoAllocGroup = 8;
+constexpr int kNoAllocBlock = 128;
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+__global__ void k_noalloc_maxdeg(const uint64_t* __restrict__ rp, uint32_t n, unsigned int* out) {
+  unsigned int m = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    uint64_t d = rp[v + 1] - rp[v];
+    m = max(m, (unsigned int)min(d, (uint64_t)0xffffffffu));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(FULL, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+// The batched form's depth-first enumeration for one graph with 64-bit row
+// pointers: work item i is root vertex i; level buffers in `base`.
+template <int G>
+__global__ void k_noalloc_dfs(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ cols, uint32_t n,
+                              int32_t query, uint32_t cap, uint32_t nbuf, uint32_t* base) {
+  Tile<G> t;
+  const uint32_t gid = blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
+  uint32_t* scratch = base + kNoAllocHeader + (size_t)gid * nbuf * cap;
+  unsigned int* next = base;
+  unsigned long long* total = reinterpret_cast<unsigned long long*>(base + 2);
+  const BProg& P = c_prog[query];
+  const int last = P.n - 1;
+  while (true) {
+    uint32_t it = 0;
+    if (t.lane == 0) it = atomicAdd(next, 1u);
+    it = t.bcast(it);
+    if (it >= n) break;
+    uint32_t M[BMAXV];
+    const uint32_t* sptr[BMAXV];
+    uint32_t slen[BMAXV], idx[BMAXV];
+    M[0] = it;
+    unsigned long long local = 0;
+    int level = 1;
+    if (level == last) {
+      LevelSet<G>(t, P.lv[1], M, rp, cols, sptr, slen, nullptr, nullptr, P.pair, &local);
+    } else {
+      uint32_t* out = P.buffered[1] ? scratch + P.buf_slot[1] * cap : nullptr;
+      slen[1] = LevelSet<G>(t, P.lv[1], M, rp, cols, sptr, slen, out, &sptr[1], false, nullptr);
+      idx[1] = 0;
+      while (level >= 1) {
+        if (idx[level] < slen[level]) {
+          M[level] = sptr[level][idx[level]];
+          ++idx[level];
+          const int nx = level + 1;
+          if (nx == last) {
+            LevelSet<G>(t, P.lv[nx], M, rp, cols, sptr, slen, nullptr, nullptr, P.pair, &local);
+          } else {
+            uint32_t* o2 = P.buffered[nx] ? scratch + P.buf_slot[nx] * cap : nullptr;
+            slen[nx] = LevelSet<G>(t, P.lv[nx], M, rp, cols, sptr, slen, o2, &sptr[nx], false, nullptr);
+            idx[nx] = 0;
+            level = nx;
+          }
+        } else {
+          --level;
+        }
+      }
+    }
+    if (t.lane == 0 && local) atomicAdd(total, local);
+  }
+}
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (the symbol's host-side name is not a device address).
+uint32_t* NoAllocScratch(int device) {
+  static std::mutex mu;
+  static uint32_t* base[64] = {nullptr};
+  if (device < 0 || device >= 64) Fail(SME_ERR_NO_DEVICE, "device ordinal out of range");
+  std::lock_guard<std::mutex> l(mu);
+  if (!base[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      Fail(SME_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+    base[device] = static_cast<uint32_t*>(p);
+  }
+  return base[device];
+}
+
+uint64_t CountNoAlloc(const uint64_t* d_rp, const uint32_t* d_cols, uint64_t n, int32_t q) {
+  if (q < 0 || q >= SME_NUM_QUERIES) Fail(SME_ERR_UNSUPPORTED_QUERY, "query_type must be 0..13");
+  if (n >= (1ULL << 31)) Fail(SME_ERR_INVALID_ARG, "sme_count_noalloc: n must be below 2^31");
+  if (n > 0 && (!d_rp || !d_cols)) Fail(SME_ERR_INVALID_ARG, "sme_count_noalloc: null device CSR");
+  int device = 0;
+  BCK(cudaGetDevice(&device));
+  uint32_t* base = NoAllocScratch(device);
+  UploadPrograms(device);
+  BCK(cudaMemsetAsync(base, 0, kNoAllocHeader * sizeof(uint32_t), 0));
+  if (n == 0) {
+    BCK(cudaStreamSynchronize(0));
+    return 0;
+  }
+  const uint32_t nv = (uint32_t)n;
+  int sms = 148;
+  BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  k_noalloc_maxdeg<<<sms * 4, 256, 0, 0>>>(d_rp, nv, base + 4);
+  uint32_t maxdeg = 0;
+  BCK(cudaMemcpy(&maxdeg, base + 4, sizeof(maxdeg), cudaMemcpyDeviceToHost));
+  if (maxdeg > kNoAllocMaxDegree)
+    Fail(SME_ERR_CAPACITY, "sme_count_noalloc: maximum degree " + std::to_string(maxdeg) +
+                               " exceeds the allocation-free limit " + std::to_string(kNoAllocMaxDegree));
+  const uint32_t nbuf = (uint32_t)MaxBuffers({q});
+  const uint32_t cap = std::max<uint32_t>(maxdeg, 1);
+  const size_t groups_fit = (kNoAllocWords - kNoAllocHeader) / ((size_t)nbuf * cap);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_noalloc_dfs<kNoAllocGroup>, kNoAllocBlock, 0);
+  const size_t gpb = kNoAllocBlock / kNoAllocGroup;
+  const size_t grid = std::max<size_t>(1, std::min<size_t>((size_t)std::max(1, per_sm) * sms, groups_fit / gpb));
+  k_noalloc_dfs<kNoAllocGroup><<<(unsigned)grid, kNoAllocBlock, 0, 0>>>(d_rp, d_cols, nv, q, cap, nbuf, base);
+  uint64_t total = 0;
+  BCK(cudaMemcpy(&total, base + 2, sizeof(total), cudaMemcpyDeviceToHost));
+  BCK(cudaGetLastError());
+  return total;
 }
 
 }  // namespace
@@ -594,6 +723,14 @@ sme_status sme_batch_describe(const sme_batch_plan* p, int32_t* g, int32_t* bloc
 sme_status sme_batch_free(sme_batch_plan* p) {
   delete p;
   return SME_OK;
+}
+
+// Allocation-free count on a caller-owned device CSR (see include/sme.h): the
+// only device memory touched besides the caller's is g_noalloc_scratch.
+sme_status sme_count_noalloc(const uint64_t* d_row_ptrs, const uint32_t* d_cols, uint64_t n, int32_t query_type,
+                             uint64_t* count) {
+  if (!count) return SME_ERR_INVALID_ARG;
+  return BGuard([&] { *count = CountNoAlloc(d_row_ptrs, d_cols, n, query_type); });
 }
 
 sme_status sme_batch_count(sme_graph* const* graphs, const int32_t* queries, uint64_t num,
