@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--load", type=float, default=0.8, help="open-loop arrival rate / plain capacity")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--granularity", type=int, default=0, help="0 auto, 1 warp per path, 2 flattened")
+    ap.add_argument("--granularity", type=int, default=0, help="0 auto (specialised warp per path), 1 warp per path generic, 2 flattened, 3 specialised at six blocks per SM")
     ap.add_argument("--list-only", action="store_true", help="no hub bitmaps (comparison)")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()

@@ -76,7 +76,11 @@ typedef struct sme_opts {
   uint64_t mem_limit_bytes;/* device budget for frontiers+graph; 0 = auto    */
   uint64_t root_begin;     /* first-level vertex range [begin,end) (a task   */
   uint64_t root_end;       /*  of IntraPartScheduler); end==0 means all      */
-  int32_t warp_granularity;/* 0 auto (flattened), 1 warp per path, 2 flattened */
+  int32_t warp_granularity;/* intersection launch shape: 0 auto (warp per
+                              path, specialised on list count, tuned
+                              occupancy), 1 warp per path generic,
+                              2 flattened (32 paths per warp), 3 as 0 with
+                              six blocks per SM throughout                  */
   int32_t list_only;       /* 1: membership by binary search only, no hub
                               bitmaps (comparison knob)                      */
   uint32_t root_stride;    /* roots are root_begin, +stride, ... < root_end

@@ -210,7 +210,11 @@ __global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __res
 // into a partner set), MODE 2 stores only the per-path count.  MINB is the
 // minimum resident blocks per SM asked of the register allocator (the
 // kernels are latency bound: more resident warps, more searches in flight).
-template <int MODE, int MINB = 1>
+// NLM bounds the lists a step intersects (backward lists + cached set), so a
+// step with two or three lists keeps fewer values live; NEX = 0 is for steps
+// without `!=` conditions (no exclusion array).  The launcher guarantees
+// both bounds.
+template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV>
 __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
     uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
@@ -224,12 +228,12 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
   const uint64_t base = b0 == 0 ? 0 : est_incl[b0 - 1];
 
   for (uint32_t p = gw; p < F.P; p += nw) {
-    const uint32_t* L[MAXV];
-    const uint32_t* B[MAXV];  // hub bitmap of the list (null: binary search)
-    uint32_t N[MAXV];
+    const uint32_t* L[NLM];
+    const uint32_t* B[NLM];  // hub bitmap of the list (null: binary search)
+    uint32_t N[NLM];
     int nl = 0;
 #pragma unroll
-    for (int i = 0; i < MAXV; ++i) {
+    for (int i = 0; i < NLM; ++i) {
       B[i] = nullptr;
       if (i < s.nconn) {
         uint32_t v = F.inst[s.conn[i]][p];
@@ -242,20 +246,20 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     }
     if (s.reuse >= 0) {
 #pragma unroll
-      for (int i = 0; i < MAXV; ++i)
+      for (int i = 0; i < NLM; ++i)
         if (i == nl) GetSet(F, s.reuse, p, L[i], N[i]);
       ++nl;
     }
     if (lane == 0) {
       uint64_t b = 12ULL * s.nconn;
 #pragma unroll
-      for (int i = 0; i < MAXV; ++i)
+      for (int i = 0; i < NLM; ++i)
         if (i < nl) b += 4ULL * N[i];
       bytes += b;
     }
     // pivot to slot 0
 #pragma unroll
-    for (int i = 1; i < MAXV; ++i) {
+    for (int i = 1; i < NLM; ++i) {
       if (i < nl && N[i] < N[0]) {
         const uint32_t* tp = L[0];
         L[0] = L[i];
@@ -268,7 +272,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
         N[i] = tn;
       }
     }
-    Bounds bd = MakeBounds(s.cond, F, p);
+    BoundsT<NEX> bd = MakeBounds<NEX>(s.cond, F, p);
     uint32_t r0 = 0, r1 = 0;
     if (nl > 0) Range(L[0], N[0], bd, r0, r1);
 
@@ -295,19 +299,19 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     uint32_t WN = 0;
     if (MODE == 1 && s.with_u >= 0) GetSet(F, s.with_u, p, W, WN);
 
-    uint32_t cur[MAXV];
+    uint32_t cur[NLM];
 #pragma unroll
-    for (int i = 0; i < MAXV; ++i) cur[i] = 0;
+    for (int i = 0; i < NLM; ++i) cur[i] = 0;
     uint32_t written = 0;
     for (uint32_t bi = r0; bi < r1; bi += 32) {
       uint32_t i = bi + lane;
       bool ok = i < r1;
       uint32_t x = ok ? __ldg(L[0] + i) : 0;
 #pragma unroll
-      for (int k = 0; k < MAXV; ++k)
+      for (int k = 0; k < NEX; ++k)
         if (k < bd.nne && x == bd.ne[k]) ok = false;
 #pragma unroll
-      for (int j = 1; j < MAXV; ++j) {
+      for (int j = 1; j < NLM; ++j) {
         if (j < nl && ok) {
           if (B[j]) {
             ok = BitTest(B[j], x);
@@ -1131,23 +1135,47 @@ class Executor {
   }
   unsigned WarpGrid(uint64_t paths) const { return Grid(paths * 32, WARP_BLOCK); }
 
-  // Intersection launch: warp per path (granularity 1) or flattened over 32
-  // paths per warp (default).
+  template <int MODE, int MINB, int NLM>
+  void LaunchWarp(bool ne, const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est, uint32_t b0,
+                  uint64_t* ptr, uint32_t* cnt, uint32_t* data, uint64_t cap, unsigned long long* acc,
+                  uint32_t* err) {
+    if (ne)
+      k_compute<MODE, MINB, NLM, MAXV><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data,
+                                                                             cap, acc, err);
+    else
+      k_compute<MODE, MINB, NLM, 0><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap,
+                                                                          acc, err);
+  }
+
+  // Intersection launch: warp per path, specialised (granularity 0 auto, 3),
+  // warp per path generic (1) or flattened over 32 paths per warp (2).
   template <int MODE>
   void Compute(const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est, uint32_t b0, uint64_t* ptr,
                uint32_t* cnt, uint32_t* data, uint64_t cap) {
     unsigned long long* acc = ctrl_;
     uint32_t* err = (uint32_t*)(ctrl_ + 3);
     Timed t = TimerStart();
-    // granularity 0 (auto): steps that intersect a cached set (short pivots)
-    // use the flattened kernel, the others warp per path
-    int gran = gran_ ? gran_ : (ds.reuse >= 0 ? 2 : 3);
-    if (gran == 1)
+    const int gran = gran_;
+    if (gran == 0 || gran == 3) {
+      // warp per path, specialised on the number of intersected lists and
+      // on the presence of `!=` conditions; fewer live values let more warps
+      // reside, which is what counts: the searches are L2-latency bound.
+      // Auto: eight blocks per SM for two or three lists, six otherwise
+      // (measured fastest on every plan at R-MAT s20); 3: six throughout.
+      const int nl = ds.nconn + (ds.reuse >= 0 ? 1 : 0);
+      bool ne = false;
+      for (int i = 0; i < ds.cond.n; ++i) ne |= ds.cond.op[i] == 2;
+      const bool dense = gran == 0;
+      if (nl <= 2)
+        dense ? LaunchWarp<MODE, 8, 2>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err)
+              : LaunchWarp<MODE, 6, 2>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+      else if (nl <= 3)
+        dense ? LaunchWarp<MODE, 8, 3>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err)
+              : LaunchWarp<MODE, 6, 3>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+      else
+        LaunchWarp<MODE, 6, MAXV>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+    } else if (gran == 1)
       k_compute<MODE><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
-    else if (gran == 3)
-      k_compute<MODE, 4><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
-    else if (gran == 4)
-      k_compute<MODE, 6><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
     else
       k_compute_flat<MODE><<<WarpGrid((F.P + 31) / 32), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data,
                                                                               cap, acc, err);

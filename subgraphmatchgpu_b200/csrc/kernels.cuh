@@ -106,15 +106,21 @@ __device__ __forceinline__ uint32_t LowerBound(const uint32_t* __restrict__ a, u
 }
 
 // Conditions of a candidate against materialised vertices reduce, on a sorted
-// list, to an interval [lo, hi) minus up to MAXV excluded values.
-struct Bounds {
+// list, to an interval [lo, hi) minus up to NE excluded values.  NE = 0 is
+// for steps whose conditions hold no `!=` (the caller checks): the exclusion
+// array then takes no registers.
+template <int NE>
+struct BoundsT {
   uint64_t lo, hi;
-  uint32_t ne[MAXV];
+  uint32_t ne[NE > 0 ? NE : 1];
   int nne;
 };
+using Bounds = BoundsT<MAXV>;
 
-__device__ __forceinline__ Bounds MakeBounds(const DCond& c, const DFront& F, uint32_t p) {
-  Bounds b;
+template <int NE = MAXV>
+__device__ __forceinline__ BoundsT<NE> MakeBounds(const DCond& c, const DFront& F, uint32_t p) {
+  static_assert(NE == 0 || NE == MAXV, "exclusion slots: none or one per condition");
+  BoundsT<NE> b;
   b.lo = 0;
   b.hi = 1ULL << 32;
   b.nne = 0;
@@ -126,7 +132,7 @@ __device__ __forceinline__ Bounds MakeBounds(const DCond& c, const DFront& F, ui
         b.hi = min(b.hi, (uint64_t)v);
       } else if (c.op[i] == 1) {
         b.lo = max(b.lo, (uint64_t)v + 1);
-      } else {
+      } else if (NE > 0) {
         b.ne[b.nne++] = v;
       }
     }
@@ -134,7 +140,8 @@ __device__ __forceinline__ Bounds MakeBounds(const DCond& c, const DFront& F, ui
   return b;
 }
 
-__device__ __forceinline__ void Range(const uint32_t* a, uint32_t n, const Bounds& b, uint32_t& r0,
+template <int NE>
+__device__ __forceinline__ void Range(const uint32_t* a, uint32_t n, const BoundsT<NE>& b, uint32_t& r0,
                                       uint32_t& r1) {
   if (b.lo >= b.hi) {
     r0 = r1 = 0;
@@ -146,11 +153,12 @@ __device__ __forceinline__ void Range(const uint32_t* a, uint32_t n, const Bound
 }
 
 // Positions (ascending) of excluded values present in a[r0,r1).
-__device__ __forceinline__ int Exclusions(const uint32_t* a, uint32_t r0, uint32_t r1, const Bounds& b,
+template <int NE>
+__device__ __forceinline__ int Exclusions(const uint32_t* a, uint32_t r0, uint32_t r1, const BoundsT<NE>& b,
                                           uint32_t* ex) {
   int k = 0;
 #pragma unroll
-  for (int i = 0; i < MAXV; ++i) {
+  for (int i = 0; i < NE; ++i) {
     if (i < b.nne) {
       uint32_t pos = r0 + LowerBound(a + r0, r1 - r0, b.ne[i]);
       if (pos < r1 && __ldg(a + pos) == b.ne[i]) ex[k++] = pos;
