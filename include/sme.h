@@ -140,6 +140,22 @@ sme_status sme_graph_write_bin(const sme_graph* g, const char* path);
 sme_status sme_graph_preprocess(sme_graph* g);
 /* GraphIO::Validate: sorted, no self loop, no parallel edge, no dangling. */
 sme_status sme_graph_validate(const sme_graph* g);
+/* Degree-ordered copy of `g` in `*out`: vertices renumbered by (degree, id)
+ * ascending, lists sorted.  A renumbering is an isomorphism, so every count
+ * is unchanged; under the clique queries' total order the candidate sets
+ * N(u) ∩ {> u} then hold only higher-degree neighbours.  orient = 1 also
+ * keeps each edge once, towards the higher new id (half the lists); an
+ * oriented graph counts only the clique queries 0, 3, 7, 11 with symmetry
+ * breaking on (others return SME_ERR_UNSUPPORTED_QUERY) and cannot be
+ * preprocessed.  new_to_old (n entries, may be NULL) receives each new id's
+ * original id, to map enumerated instances back.
+ * No counterpart in the reference, which stores both directions and relies
+ * on the `<` conditions; the R-MAT s22 clique configuration of this path asks
+ * for the degree-ordered orientation. */
+sme_status sme_graph_degree_order(const sme_graph* g, int32_t orient, sme_graph** out,
+                                  uint32_t* new_to_old);
+/* 1 when `g` was made by sme_graph_degree_order with orient = 1. */
+int32_t sme_graph_is_oriented(const sme_graph* g);
 /* Copies the CSR to device memory of `device` and keeps it there; later runs
  * on that device reuse it (inputs resident in HBM). */
 sme_status sme_graph_to_device(sme_graph* g, int device);

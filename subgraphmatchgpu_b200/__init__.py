@@ -99,6 +99,8 @@ SIGNATURES = {
     "sme_graph_write_bin": (C.c_int, [_P, C.c_char_p]),
     "sme_graph_preprocess": (C.c_int, [_P]),
     "sme_graph_validate": (C.c_int, [_P]),
+    "sme_graph_degree_order": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_void_p), C.c_void_p]),
+    "sme_graph_is_oriented": (C.c_int32, [_P]),
     "sme_graph_to_device": (C.c_int, [_P, C.c_int]),
     "sme_graph_release_device": (C.c_int, [_P]),
     "sme_graph_free": (C.c_int, [_P]),
@@ -261,6 +263,19 @@ class Graph:
 
     def validate(self) -> None:
         _check(lib().sme_graph_validate(self._h))
+
+    def degree_order(self, orient: bool = False):
+        """(degree-ordered copy, new_to_old uint32[n]); `orient` keeps each
+        edge once, towards the higher id (clique queries only)."""
+        n = self.info()[0]
+        new_to_old = np.zeros(max(n, 1), np.uint32)
+        h = C.c_void_p()
+        _check(lib().sme_graph_degree_order(self._h, int(orient), C.byref(h), new_to_old.ctypes.data))
+        return Graph(h.value), new_to_old[:n]
+
+    @property
+    def oriented(self) -> bool:
+        return bool(lib().sme_graph_is_oriented(self._h))
 
     def to_device(self, device: int = 0) -> None:
         _check(lib().sme_graph_to_device(self._h, device))

@@ -701,6 +701,12 @@ sme_status sme_batch_prepare(sme_graph* const* graphs, const int32_t* queries, u
     sme_batch_opts o;
     sme_batch_opts_default(&o);
     if (opts) o = *opts;
+    // the batched plan extends in identity order with whole-ordered
+    // conditions: on an oriented graph only the ordered cliques count right
+    for (uint64_t i = 0; i < num; ++i)
+      if (graphs[i] && graphs[i]->g.oriented && !IsOrderedClique(Query(queries[i], true)))
+        Fail(SME_ERR_UNSUPPORTED_QUERY, "graph " + std::to_string(i) +
+                                            " is oriented: only the clique queries (0, 3, 7, 11) count on it");
     std::unique_ptr<sme_batch_plan> p(new sme_batch_plan());
     Prepare(graphs, queries, num, o, p.get());
     *out = p.release();

@@ -72,6 +72,7 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
   CheckOpts(o);
   auto t0 = std::chrono::steady_clock::now();
   Program prog = Compile(o, enumerate);
+  if (g->g.oriented) RequireOrientable(prog, o.enable_ordering != 0);
   CtxSlot& slot = SlotFor(o.device);
   std::lock_guard<std::mutex> lock(slot.mu);
   if (!slot.ctx || (o.mem_limit_bytes && slot.bytes != o.mem_limit_bytes)) {
@@ -227,6 +228,7 @@ sme_status sme_graph_write_bin(const sme_graph* g, const char* path) {
 sme_status sme_graph_preprocess(sme_graph* g) {
   if (!g) return SME_ERR_INVALID_ARG;
   return Guard([&] {
+    if (g->g.oriented) Fail(SME_ERR_INVALID_ARG, "an oriented graph cannot be preprocessed");
     if (g->g.dev) {
       FreeDeviceGraph(g->g.dev);
       g->g.dev = nullptr;
@@ -234,6 +236,20 @@ sme_status sme_graph_preprocess(sme_graph* g) {
     Preprocess(g->g);
   });
 }
+
+sme_status sme_graph_degree_order(const sme_graph* g, int32_t orient, sme_graph** out, uint32_t* new_to_old) {
+  if (!g || !out || (orient != 0 && orient != 1)) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    if (g->g.oriented) Fail(SME_ERR_INVALID_ARG, "the graph is oriented already");
+    std::unique_ptr<sme_graph> r(new sme_graph());
+    std::vector<uintV> map;
+    DegreeOrder(g->g, orient != 0, r->g, new_to_old ? &map : nullptr);
+    if (new_to_old) std::copy(map.begin(), map.end(), new_to_old);
+    *out = r.release();
+  });
+}
+
+int32_t sme_graph_is_oriented(const sme_graph* g) { return g && g->g.oriented ? 1 : 0; }
 
 sme_status sme_graph_validate(const sme_graph* g) {
   if (!g) return SME_ERR_INVALID_ARG;

@@ -36,7 +36,7 @@ void Help() {
                "-e PARTITION_FILENAME -p PARTITION_NUM -t THREAD_NUM -v DEVICE_NUM "
                "-m EXECUTE_MODE -o VARIANT [ -l MATERIALIZE -r ENABLE_ORDERING -c "
                "LAZY_TRAVERSAL_COMPRESS_LEVEL -x GPU_LIGHT_ITP_VARIANT -y GPU_LIGHT_EXT_VARIANT"
-               " -g REUSE_AUTOGEN -b ROOT_BEGIN -n ROOT_END -M MEM_LIMIT_MB ]\n";
+               " -g REUSE_AUTOGEN -b ROOT_BEGIN -n ROOT_END -M MEM_LIMIT_MB -O DEGREE_ORDER ]\n";
   std::cout << "ALGORITHM: ,GPU_GPSM=4,GPU_GPSM_REUSE=5,GPU_LIGHT=6\n";
   std::cout << "QUERY: Q0 (TRIANGLE) 0, Q1 (square) 1, Q2 (chordal square) 2, Q3 (4 clique) 3, "
                "Q4 (house) 4, Q5 (quad triangle) 5, Q6 (near5clique) 6, Q7 (5 clique) 7, "
@@ -47,6 +47,8 @@ void Help() {
                "COMPRESS_LEVEL_NON_MATERIALIZE=1, COMPRESS_LEVEL_NON_MATERIALIZE_OPT=2, "
                "COMPRESS_LEVEL_SPECIAL(DEFAULT)=3\n";
   std::cout << "GPU_LIGHT_EXT_VARIANT: EXT_CACHE(DEFAULT)=0, EXT_UMA=1\n";
+  std::cout << "DEGREE_ORDER: none(DEFAULT)=0, renumber by degree=1, renumber and orient (clique "
+               "queries 0/3/7/11 only)=2\n";
 }
 
 int Die(const char* what, sme_status st) {
@@ -78,6 +80,7 @@ int main(int argc, char** argv) {
   o.root_begin = (uint64_t)a.Int("-b", 0);
   o.root_end = (uint64_t)a.Int("-n", 0);
   o.mem_limit_bytes = (uint64_t)a.Int("-M", 0) << 20;
+  const int degree_order = (int)a.Int("-O", 0);
 
   std::cout << "filename=" << filename << ",directed=" << directed << ",algo=" << o.algo
             << ",query_type=" << o.query_type << std::endl;
@@ -96,6 +99,16 @@ int main(int argc, char** argv) {
   sme_graph* g = nullptr;
   sme_status st = sme_graph_load(filename.c_str(), directed, &g);
   if (st != SME_OK) return Die("graph load", st);
+  if (degree_order == 1 || degree_order == 2) {
+    sme_graph* d = nullptr;
+    st = sme_graph_degree_order(g, degree_order - 1, &d, nullptr);
+    if (st != SME_OK) return Die("degree order", st);
+    sme_graph_free(g);
+    g = d;
+  } else if (degree_order != 0) {
+    std::cerr << "-O must be 0, 1 or 2" << std::endl;
+    return 1;
+  }
   uint64_t n = 0, m = 0, dmax = 0;
   sme_graph_info(g, &n, &m, &dmax);
   std::cout << "vertex_count=" << n << ",edge_count=" << m << ",max_degree=" << dmax << std::endl;

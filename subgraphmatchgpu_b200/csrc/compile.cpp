@@ -316,6 +316,32 @@ Program Compile(const sme_opts& o, bool enumerate) {
   return p;
 }
 
+bool IsOrderedClique(const Query& q) {
+  if (!q.enable_ordering) return false;
+  for (int u = 0; u < q.n; ++u) {
+    if ((int)q.con[u].size() != q.n - 1) return false;
+    if (u + 1 < q.n && GetConditionType((uintV)u, (uintV)(u + 1), q.order) != LESS_THAN) return false;
+  }
+  return true;
+}
+
+void RequireOrientable(const Program& p, bool enable_ordering) {
+  Query q(p.query_type, enable_ordering);
+  if (!IsOrderedClique(q))
+    Fail(SME_ERR_UNSUPPORTED_QUERY,
+         "an oriented graph holds each edge once: only the clique queries (0, 3, 7, 11) with symmetry "
+         "breaking count on it");
+  // every list a step reads must belong to a vertex that precedes u in the
+  // total order, so the forward list holds all of u's candidates
+  for (const Step& s : p.steps) {
+    auto before = [&](uint8_t w) { return p.out_slot[w] < p.out_slot[s.u]; };
+    for (uint8_t w : s.conn)
+      if (!before(w)) Fail(SME_ERR_UNSUPPORTED_QUERY, "plan reads a list against the orientation");
+    for (uint8_t w : s.full_conn)
+      if (!before(w)) Fail(SME_ERR_UNSUPPORTED_QUERY, "plan reads a list against the orientation");
+  }
+}
+
 std::string Program::Describe() const {
   std::ostringstream os;
   os << "program Q" << query_type << " algo=" << algo << (enumerate ? " enumerate" : " count") << "\n";

@@ -128,6 +128,7 @@ struct sme_server {
       try {
         const HostGraph& hg = r.attached ? r.attached->g : resident[r.gid]->g;
         Program prog = Compile(r.opts, false);
+        if (hg.oriented) RequireOrientable(prog, r.opts.enable_ordering != 0);
         DeviceGraph* dg = hg.dev;
         bool temp = false;
         if (!dg || dg->device != o.device) {

@@ -185,6 +185,53 @@ void Validate(const HostGraph& g) {
                                   " unsorted=" + std::to_string(unsorted));
 }
 
+// Renumbers vertices by (degree, id) ascending, so that under a total order
+// of the pattern (the clique queries) every candidate set N(u) ∩ {> u} holds
+// only neighbours of higher degree — the degree orientation that bounds those
+// sets by O(sqrt(m)).  A counting sort by degree keeps ties in id order, so
+// the result is deterministic.  `orient` keeps, per vertex, only the
+// neighbours with a higher new id (each undirected edge once).
+void DegreeOrder(const HostGraph& in, bool orient, HostGraph& out, std::vector<uintV>* new_to_old) {
+  const uint64_t n = in.n;
+  uint64_t dmax = 0;
+  for (uint64_t u = 0; u < n; ++u) dmax = std::max<uint64_t>(dmax, in.row_ptrs[u + 1] - in.row_ptrs[u]);
+  std::vector<uint64_t> start(dmax + 2, 0);
+  for (uint64_t u = 0; u < n; ++u) ++start[in.row_ptrs[u + 1] - in.row_ptrs[u] + 1];
+  for (uint64_t d = 0; d <= dmax; ++d) start[d + 1] += start[d];
+  std::vector<uintV> old_of(n), new_of(n);
+  for (uint64_t u = 0; u < n; ++u) {
+    uint64_t x = start[in.row_ptrs[u + 1] - in.row_ptrs[u]]++;
+    old_of[x] = (uintV)u;
+    new_of[u] = (uintV)x;
+  }
+  std::vector<uintE> r(n + 1, 0);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (uint64_t x = 0; x < n; ++x) {
+    const uint64_t v = old_of[x];
+    uintE k = in.row_ptrs[v + 1] - in.row_ptrs[v];
+    if (orient) {
+      k = 0;
+      for (uintE j = in.row_ptrs[v]; j < in.row_ptrs[v + 1]; ++j) k += new_of[in.cols[j]] > x;
+    }
+    r[x + 1] = k;
+  }
+  for (uint64_t x = 0; x < n; ++x) r[x + 1] += r[x];
+  std::vector<uintV> c(r[n]);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (uint64_t x = 0; x < n; ++x) {
+    const uint64_t v = old_of[x];
+    uintE o = r[x];
+    for (uintE j = in.row_ptrs[v]; j < in.row_ptrs[v + 1]; ++j) {
+      uintV w = new_of[in.cols[j]];
+      if (!orient || w > x) c[o++] = w;
+    }
+    std::sort(c.begin() + r[x], c.begin() + r[x + 1]);
+  }
+  out.Adopt(std::move(r), std::move(c));
+  out.oriented = orient;
+  if (new_to_old) *new_to_old = std::move(old_of);
+}
+
 void BuildFromEdges(uint64_t n, std::vector<std::pair<uintV, uintV>>& edges, HostGraph& g) {
   std::vector<uintE> r(n + 1, 0);
   for (auto& p : edges) {

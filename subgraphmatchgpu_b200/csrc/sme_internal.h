@@ -37,6 +37,7 @@ struct HostGraph {
   uintE* row_ptrs = nullptr;
   uintV* cols = nullptr;
   bool borrowed = false;
+  bool oriented = false;       // each edge once, towards the higher id
   std::vector<uintE> row_store;
   std::vector<uintV> col_store;
   DeviceGraph* dev = nullptr;  // resident device copy (may be null)
@@ -53,6 +54,9 @@ void Validate(const HostGraph& g);
 // then applies Preprocess().
 void BuildFromEdges(uint64_t n, std::vector<std::pair<uintV, uintV>>& edges,
                     HostGraph& g);
+// Degree-ordered copy (vertices renumbered by (degree, id) ascending),
+// optionally oriented towards the higher id; new_to_old[new] = old id.
+void DegreeOrder(const HostGraph& in, bool orient, HostGraph& out, std::vector<uintV>* new_to_old);
 void GenerateRmat(int scale, int edge_factor, double a, double b, double c,
                   uint64_t seed, HostGraph& g);
 void GenerateER(uint64_t n, double avg_degree, uint64_t seed, HostGraph& g);
@@ -181,6 +185,11 @@ struct Program {
 };
 // Builds the level program of a query under one of the three GPU plans.
 Program Compile(const sme_opts& o, bool enumerate);
+// A clique query whose symmetry breaking is the total order u0 < u1 < ...
+bool IsOrderedClique(const Query& q);
+// Fails unless `p` counts correctly on an oriented graph: an ordered clique
+// whose every adjacency list read belongs to an earlier vertex of the order.
+void RequireOrientable(const Program& p, bool enable_ordering);
 
 }  // namespace sme
 

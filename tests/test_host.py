@@ -134,3 +134,81 @@ def test_compiled_programs_are_consistent():
             lines = prog.strip().splitlines()[1:]
             assert lines[0].split(":")[1].strip().startswith("INIT")
             assert re.search(r"(COMPUTE_COUNT|COUNT)\(", lines[-1])
+
+
+CLIQUES = (0, 3, 7, 11)
+
+
+def test_degree_order_is_an_isomorphism_sorted_by_degree():
+    g = sme.Graph.rmat(10, 8, seed=5)
+    rp, cl = g.csr()
+    d, new_to_old = g.degree_order()
+    assert not d.oriented
+    drp, dcl = d.csr()
+    n = len(rp) - 1
+    assert len(drp) == n + 1 and len(dcl) == len(cl)
+    assert sorted(new_to_old.tolist()) == list(range(n))
+    deg_old, deg_new = np.diff(rp).astype(np.int64), np.diff(drp).astype(np.int64)
+    assert np.array_equal(deg_new, deg_old[new_to_old])
+    keys = deg_new.astype(np.int64) * n + new_to_old.astype(np.int64)
+    assert np.all(np.diff(keys) > 0)  # (degree, original id) ascending
+    d.validate()
+    old_edges = set(zip(np.repeat(np.arange(n), deg_old).tolist(), cl.tolist()))
+    new_edges = zip(new_to_old[np.repeat(np.arange(n), deg_new)].tolist(), new_to_old[dcl].tolist())
+    assert set(new_edges) == old_edges
+
+
+@pytest.mark.parametrize("name", ["rmat_s10_ef8", "ba_n600_m4", "er_n64_d12"])
+def test_degree_order_preserves_every_count(golden, name):
+    import oracle_py as O
+    rp, cl = O.read_bin(golden_graph_path(name))
+    d, _ = sme.Graph.from_csr(rp, cl).degree_order()
+    drp, dcl = d.csr()
+    for q, want in golden[name]["counts"].items():
+        if want > 5e7:
+            continue
+        assert O.count(drp, dcl, int(q)) == want, (name, q)
+
+
+def test_oriented_graph_keeps_each_edge_once_towards_higher_id():
+    g = sme.Graph.rmat(10, 8, seed=5)
+    _, cl = g.csr()
+    o, _ = g.degree_order(orient=True)
+    assert o.oriented
+    orp, ocl = o.csr()
+    assert 2 * len(ocl) == len(cl)
+    src = np.repeat(np.arange(len(orp) - 1), np.diff(orp).astype(np.int64))
+    assert np.all(ocl > src)
+    with pytest.raises(sme.SmeError) as e:
+        o.preprocess()
+    assert e.value.status == 1
+    with pytest.raises(sme.SmeError) as e:
+        o.degree_order()
+    assert e.value.status == 1
+
+
+@pytest.mark.parametrize("q", [1, 2, 4, 5, 6, 8, 9, 10, 12, 13])
+def test_oriented_graph_rejects_non_clique_queries(q):
+    # checked at plan time, before any device call
+    o, _ = sme.Graph.rmat(8, 8, seed=2).degree_order(orient=True)
+    for algo in (4, 5, 6):
+        with pytest.raises(sme.SmeError) as e:
+            o.count(q, algo)
+        assert e.value.status == 6, (q, algo)
+    with pytest.raises(sme.SmeError) as e:
+        o.count(3, 6, enable_ordering=0)
+    assert e.value.status == 6
+
+
+def test_clique_plans_read_lists_along_the_orientation():
+    # every clique plan (all three algorithms, every LIGHT compress level)
+    # passes the plan-time orientation check: the count on an oriented graph
+    # reaches the device stage (without a GPU: a device error, not status 6)
+    o, _ = sme.Graph.rmat(8, 8, seed=2).degree_order(orient=True)
+    for q in CLIQUES:
+        for algo, kw in ((4, {}), (5, {}), (5, {"reuse_autogen": 1})) + tuple((6, {"compress_level": c})
+                                                                           for c in range(4)):
+            try:
+                o.count(q, algo, **kw)
+            except sme.SmeError as e:
+                assert e.status != 6, (q, algo, kw, str(e))
