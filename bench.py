@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--granularity", type=int, default=0, help="0 auto (specialised warp per path), 1 warp per path generic, 2 flattened, 3 specialised at six blocks per SM")
     ap.add_argument("--list-only", action="store_true", help="no hub bitmaps (comparison)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-s22", action="store_true", help="skip the R-MAT s22 4-clique leg")
     return ap.parse_args()
 
 
@@ -277,6 +278,29 @@ def bench_served(args, device):
             "counts_equal_alone_and_in_mix": same}
 
 
+def bench_s22(args, device, tune, peak):
+    """R-MAT scale 22 (edge factor 16) 4-clique under the bench's plan: device
+    time and the intersection roofline, on the graph as generated and on its
+    degree-ordered orientation (same count)."""
+    import subgraphmatchgpu_b200 as sme
+    g = sme.Graph.rmat(22, args.edge_factor, 0.57, 0.19, 0.19, seed=22)
+    o, _ = g.degree_order(orient=True)
+    out = {"workload": f"R-MAT s22 ef{args.edge_factor} seed 22 (n={g.n}, m={g.m}), 4-clique, plan algo "
+                       f"{args.algo}, IN_MEMORY_GPU, one run each"}
+    for tag, gr in (("as_generated", g), ("degree_oriented", o)):
+        gr.to_device(device)
+        c = gr.count(3, args.algo, device=device, **tune)
+        s = sme.last_stats()
+        ach = s.algorithmic_bytes / (s.kernel_ms / 1e3) / 1e9 if s.kernel_ms > 0 else 0.0
+        out[tag] = {"instances": c, "device_ms": s.device_ms, "value": c / (s.device_ms / 1e3), "unit": UNIT,
+                    "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                                 "frac": round(ach / peak, 4), "kernel_ms": s.kernel_ms,
+                                 "algorithmic_bytes": s.algorithmic_bytes, "launches": s.hot_launches}}
+        gr.release_device()
+    out["counts_equal"] = out["as_generated"]["instances"] == out["degree_oriented"]["instances"]
+    return out
+
+
 def reduce_over_ranks(dev_ms, instances, dist, device):
     """Replicas: the job's time is the slowest rank's device time, its work
     the sum of the ranks' instances (timing only; no data-path collective)."""
@@ -471,6 +495,12 @@ def main():
                 forms[name] = fn(args, local)
             except Exception as e:  # reported in the line, never dropped silently
                 forms[name] = {"error": f"{type(e).__name__}: {e}"}
+    s22 = None
+    if rank == 0 and world == 1 and not args.no_s22:
+        try:
+            s22 = bench_s22(args, local, tune, peak)
+        except Exception as e:
+            s22 = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         line = {
@@ -488,7 +518,7 @@ def main():
                                               "phase_ms": dict(zip(sme.Stats.PHASES, [round(x, 3) for x in v[2]]))}
                                      for q, v in per_query.items()}},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
-            "gpu_launches": launches, "forms": forms,
+            "gpu_launches": launches, "forms": forms, "s22_4clique": s22,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -85,7 +85,12 @@ typedef struct sme_opts {
                               bitmaps (comparison knob)                      */
   uint32_t root_stride;    /* roots are root_begin, +stride, ... < root_end
                               (0 or 1: every root); a strided task          */
-  int32_t reserved[5];
+  int32_t no_set_reuse;    /* LIGHT: 1 computes every candidate set from
+                              adjacency lists, as the reference does; 0
+                              (default) starts a set from an earlier
+                              candidate set that covers some of its lists
+                              when the conditions allow (same sets)        */
+  int32_t reserved[4];
 } sme_opts;
 
 /* Counters of the last sme_count/sme_enumerate call on this thread. */

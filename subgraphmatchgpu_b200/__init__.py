@@ -50,7 +50,8 @@ class Opts(C.Structure):
         ("compress_level", C.c_int32), ("enable_ordering", C.c_int32), ("ext_variant", C.c_int32),
         ("reuse_autogen", C.c_int32), ("device", C.c_int32), ("mem_limit_bytes", C.c_uint64),
         ("root_begin", C.c_uint64), ("root_end", C.c_uint64), ("warp_granularity", C.c_int32),
-        ("list_only", C.c_int32), ("root_stride", C.c_uint32), ("reserved", C.c_int32 * 5),
+        ("list_only", C.c_int32), ("root_stride", C.c_uint32), ("no_set_reuse", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 

@@ -194,10 +194,143 @@ Program CompileReuse(const Query& q, bool autogen, bool enumerate) {
   return p;
 }
 
+bool HasCond(const std::vector<StepCond>& v, uint8_t op, uint8_t operand) {
+  for (auto& c : v)
+    if (c.op == op && c.operand == operand) return true;
+  return false;
+}
+
+// True when every x satisfying `c` (conditions against materialised
+// vertices) also satisfies `need`.  Facts grow by transitivity through
+// materialised vertices: x > M[a] and M[a] > M[b] (a relation M[a] was
+// checked against, `known[a]`) give x > M[b]; likewise for <.  A strict
+// order against v also gives x != M[v].
+bool Implies(const std::vector<StepCond>& c, const std::vector<StepCond>& need, const std::vector<bool>& mat,
+             const std::vector<std::vector<StepCond>>& known) {
+  std::vector<StepCond> facts = c;
+  for (size_t k = 0; k < facts.size(); ++k) {
+    const StepCond f = facts[k];
+    if (f.op == NON_EQUAL || !mat[f.operand]) continue;
+    for (const StepCond& r : known[f.operand])
+      if (r.op == f.op && !HasCond(facts, f.op, r.operand)) facts.push_back(StepCond{f.op, r.operand});
+  }
+  for (const StepCond& x : need) {
+    bool ok = HasCond(facts, x.op, x.operand) ||
+              (x.op == NON_EQUAL && (HasCond(facts, LESS_THAN, x.operand) || HasCond(facts, LARGER_THAN, x.operand)));
+    if (!ok) return false;
+  }
+  return true;
+}
+
+// Candidate-set reuse for the LIGHT sequence.  The reference computes every
+// candidate set from adjacency lists.  When an earlier candidate set of w
+// was intersected from lists T ⊆ S (S = the lists of u) and every condition
+// that set was filtered by follows from u's own conditions, then
+// set(u) = set(w) ∩ lists(S \ T) under u's conditions: the same set from
+// fewer, shorter inputs.  On the clique queries this turns the k-way
+// intersection at every level into one 2-way step.  Returns, per sequence
+// entry, the vertex whose set the entry starts from (-1 none).
+std::vector<int> PlanSetReuse(const LazyPlan& lp, const Query& q, std::vector<int>& last_use_after_mat,
+                              std::vector<std::vector<uint8_t>>& covered) {
+  const size_t E = lp.exec.size();
+  std::vector<int> from(E, -1);
+  covered.assign(E, {});
+  std::vector<bool> mat(q.n, false), live(q.n, false), has(q.n, false);
+  std::vector<std::vector<uint8_t>> lists(q.n);
+  std::vector<std::vector<StepCond>> cset(q.n), known(q.n);
+  last_use_after_mat.assign(q.n, -1);
+  for (size_t i = 0; i < E; ++i) {
+    const LazyOp op = lp.exec[i].first;
+    const uint8_t u = (uint8_t)lp.exec[i].second;
+    if (op == L_MATERIALIZE) {
+      if (i > 0) {
+        known[u] = cset[u];
+        for (const StepCond& c : Conds(lp.materialize_cond[u])) known[u].push_back(c);
+      }
+      mat[u] = true;
+      live[u] = false;
+    } else if (op == L_FILTER_COMPUTE) {
+      for (const StepCond& c : Conds(lp.filter_cond[u])) cset[u].push_back(c);
+    } else if (op == L_COMPUTE || op == L_COMPUTE_PATH_COUNT || op == L_COMPUTE_COUNT) {
+      const std::vector<uint8_t> S = U8(lp.backward_conn[u]);
+      const std::vector<StepCond> C = Conds(lp.compute_cond[u]);
+      int best = -1;
+      for (int w = 0; w < q.n; ++w) {
+        if (w == u || !has[w] || !(live[w] || mat[w])) continue;
+        if (lists[w].size() < 2 || (best >= 0 && lists[w].size() <= lists[best].size())) continue;
+        bool subset = true;
+        for (uint8_t t : lists[w])
+          if (std::find(S.begin(), S.end(), t) == S.end()) subset = false;
+        if (subset && Implies(C, cset[w], mat, known)) best = w;
+      }
+      from[i] = best;
+      if (best >= 0) covered[i] = lists[best];
+      if (best >= 0 && mat[best]) last_use_after_mat[best] = (int)i;
+      if (op == L_COMPUTE) {
+        has[u] = live[u] = true;
+        lists[u] = S;
+        cset[u] = C;
+        if (best >= 0)
+          for (const StepCond& c : cset[best]) cset[u].push_back(c);
+      }
+    }
+  }
+  return from;
+}
+
+// Drops `!=` conditions that the strict ones already imply (x > M[w] with
+// M[w] > M[v] gives x != M[v]): the clique plans fill every unordered pair
+// with NON_EQUAL, yet their total order makes those checks dead.  Steps
+// without `!=` run the intersection without an exclusion array.
+void PruneImpliedExclusions(Program& p) {
+  const int n = p.n;
+  std::vector<bool> mat(n, false);
+  std::vector<std::vector<StepCond>> cset(n), known(n);
+  for (Step& s : p.steps) {
+    const uint8_t u = s.u;
+    // facts every candidate of this step satisfies besides its own `!=`
+    std::vector<StepCond> strict;
+    for (const StepCond& c : s.cond)
+      if (c.op != NON_EQUAL) strict.push_back(c);
+    if (s.kind == S_MATERIALIZE || s.kind == S_FILTER)
+      for (const StepCond& c : cset[u])
+        if (c.op != NON_EQUAL) strict.push_back(c);
+    std::vector<StepCond> kept;
+    for (const StepCond& c : s.cond) {
+      bool dead = c.op == NON_EQUAL && mat[c.operand] &&
+                  (Implies(strict, {StepCond{LESS_THAN, c.operand}}, mat, known) ||
+                   Implies(strict, {StepCond{LARGER_THAN, c.operand}}, mat, known));
+      if (!dead) kept.push_back(c);
+    }
+    // bookkeeping uses the full condition lists (facts, not checks)
+    switch (s.kind) {
+      case S_INIT:
+        mat[u] = true;
+        break;
+      case S_COMPUTE:
+        cset[u] = s.cond;
+        if (s.reuse_src >= 0)
+          for (const StepCond& c : cset[s.reuse_src]) cset[u].push_back(c);
+        break;
+      case S_FILTER:
+        for (const StepCond& c : s.cond) cset[u].push_back(c);
+        break;
+      case S_MATERIALIZE:
+        known[u] = cset[u];
+        for (const StepCond& c : s.cond) known[u].push_back(c);
+        mat[u] = true;
+        break;
+      default:
+        break;
+    }
+    s.cond = kept;
+  }
+}
+
 // LIGHT: the reference execute sequence; for enumeration the counting tail
 // is replaced by materialising every vertex (conditions recomputed by the
 // same utilities, so each pair of pattern vertices is still checked once).
-Program CompileLight(const Query& q, int compress_level, bool enumerate) {
+Program CompileLight(const Query& q, int compress_level, bool enumerate, bool set_reuse) {
   LazyPlan lp(q, compress_level);
   if (enumerate) {
     std::vector<LazyEntry> e;
@@ -227,6 +360,23 @@ Program CompileLight(const Query& q, int compress_level, bool enumerate) {
   for (int u = 0; u < q.n; ++u) p.out_slot.push_back((uint8_t)u);
   const bool direct_ok = lp.compress_level == SME_COMPRESS_SPECIAL && q.type <= 11 && q.type != 4 &&
                          q.type != 9;  // CanDirectCount, LIGHTDirectCount.cuh:13-19
+  std::vector<int> last_use(q.n, -1);
+  std::vector<int> from(lp.exec.size(), -1);
+  std::vector<std::vector<uint8_t>> covered(lp.exec.size());
+  if (set_reuse) from = PlanSetReuse(lp, q, last_use, covered);
+  // lists of a compute entry: all backward lists, or those its reused set
+  // does not cover (full_conn keeps all of them)
+  auto lists_of = [&](size_t i, uint8_t u, Step& s) {
+    s.conn = U8(lp.backward_conn[u]);
+    if (from[i] < 0) return;
+    const uint8_t w = (uint8_t)from[i];
+    s.full_conn = s.conn;
+    s.reuse_src = (int8_t)w;
+    std::vector<uint8_t> rest;
+    for (uint8_t t : s.conn)
+      if (std::find(covered[i].begin(), covered[i].end(), t) == covered[i].end()) rest.push_back(t);
+    s.conn = rest;
+  };
   for (size_t i = 0; i < lp.exec.size(); ++i) {
     LazyOp op = lp.exec[i].first;
     uint8_t u = (uint8_t)lp.exec[i].second;
@@ -239,14 +389,18 @@ Program CompileLight(const Query& q, int compress_level, bool enumerate) {
         } else {
           s.kind = S_MATERIALIZE;
           s.cond = Conds(lp.materialize_cond[u]);
-          st.DropSet(u);
+          // a set reused after this point stays with the children
+          s.keep_set = last_use[u] > (int)i;
+          if (!s.keep_set) st.DropSet(u);
+          for (int w = 0; w < q.n; ++w)
+            if (w != u && last_use[w] >= 0 && last_use[w] < (int)i) st.DropSet((uint8_t)w);
         }
         st.AddMat(u);
         break;
       case L_COMPUTE:
       case L_COMPUTE_PATH_COUNT:
         s.kind = op == L_COMPUTE ? S_COMPUTE : S_PATH_COUNT;
-        s.conn = U8(lp.backward_conn[u]);
+        lists_of(i, u, s);
         s.cond = Conds(lp.compute_cond[u]);
         st.AddSet(u);
         break;
@@ -256,7 +410,7 @@ Program CompileLight(const Query& q, int compress_level, bool enumerate) {
         break;
       case L_COMPUTE_COUNT: {
         s.kind = S_COMPUTE_COUNT;
-        s.conn = U8(lp.backward_conn[u]);
+        lists_of(i, u, s);
         s.cond = Conds(lp.compute_cond[u]);
         auto& um = lp.computed_unmaterialized[i];
         if (um.size() > 1) Fail(SME_ERR_UNSUPPORTED_QUERY, "COMPUTE_COUNT with >1 unmaterialized vertex");
@@ -300,7 +454,7 @@ Program Compile(const sme_opts& o, bool enumerate) {
     case SME_GPU_LIGHT:
       if (o.compress_level < 0 || o.compress_level > 3)
         Fail(SME_ERR_INVALID_ARG, "compress_level must be 0..3");
-      p = CompileLight(q, o.compress_level, enumerate);
+      p = CompileLight(q, o.compress_level, enumerate, o.no_set_reuse == 0);
       break;
     default:
       Fail(SME_ERR_INVALID_ARG, "algo must be 4 (GPU_GPSM), 5 (GPU_GPSM_REUSE) or 6 (GPU_LIGHT)");
@@ -308,6 +462,7 @@ Program Compile(const sme_opts& o, bool enumerate) {
   p.query_type = q.type;
   p.algo = o.algo;
   p.enumerate = enumerate;
+  PruneImpliedExclusions(p);
   for (auto& s : p.steps) {
     std::ostringstream os;
     os << KindName(s.kind) << "(" << (int)s.u << ")";

@@ -58,6 +58,17 @@ def test_light_compress_levels(graphs, golden, level):
             assert graphs[name].count(int(q), sme.GPU_LIGHT, compress_level=level) == want, (name, q, level)
 
 
+@pytest.mark.parametrize("level", [0, 3])
+def test_light_without_set_reuse(graphs, golden, level):
+    # every candidate set from adjacency lists, as the reference computes them
+    for name in ("rmat_s10_ef8", "ba_n600_m4", "k12", "er_n64_d12"):
+        for q, want in golden[name]["counts"].items():
+            if want > GPU_LIMIT:
+                continue
+            got = graphs[name].count(int(q), sme.GPU_LIGHT, compress_level=level, no_set_reuse=1)
+            assert got == want, (name, q, level)
+
+
 def test_reuse_autogen_plans(graphs, golden):
     for name in ("rmat_s10_ef8", "er_n64_d12"):
         for q, want in golden[name]["counts"].items():

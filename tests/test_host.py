@@ -212,3 +212,16 @@ def test_clique_plans_read_lists_along_the_orientation():
                 o.count(q, algo, **kw)
             except sme.SmeError as e:
                 assert e.status != 6, (q, algo, kw, str(e))
+
+
+def test_light_clique_programs_start_from_earlier_sets():
+    # 4-clique: the count step intersects set(2) = N(0) ∩ N(1) ∩ {> 1} with
+    # N(2) instead of three lists; set(2) stays with the children of M(2)
+    light = sme.plan_describe(3, 5).split("program Q")[3]
+    assert "MATERIALIZE(2) keep" in light
+    # the != conditions the total order implies are dropped
+    assert "COMPUTE_COUNT(3) conn=(2) reuse=2 cond=(>2)" in light
+    # 4-cycle: no earlier set covers two of its lists; u2 != u1 is a real check
+    q1 = sme.plan_describe(1, 5).split("program Q")[3]
+    assert "reuse=" not in q1
+    assert "COMPUTE(2) conn=(1) cond=(>0,!=1)" in q1
