@@ -75,7 +75,9 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
   if (g->g.oriented) RequireOrientable(prog, o.enable_ordering != 0);
   CtxSlot& slot = SlotFor(o.device);
   std::lock_guard<std::mutex> lock(slot.mu);
-  if (!slot.ctx || (o.mem_limit_bytes && slot.bytes != o.mem_limit_bytes)) {
+  // the arena follows each call's budget (0 = auto), so a call never runs in
+  // the smaller arena a previous call asked for
+  if (!slot.ctx || slot.bytes != o.mem_limit_bytes) {
     if (slot.ctx) DestroyContext(slot.ctx);
     slot.ctx = nullptr;
     slot.ctx = CreateContext(o.device, o.mem_limit_bytes);

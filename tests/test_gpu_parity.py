@@ -114,6 +114,16 @@ def test_small_memory_budget_forces_many_batches(graphs, golden):
             assert sme.last_stats().batches > 3
 
 
+def test_auto_budget_after_a_small_budget_call(graphs, golden):
+    # a call with the auto budget must not inherit the previous call's arena
+    g = graphs["rmat_s12_ef8"]
+    want = golden["rmat_s12_ef8"]["counts"]["3"]
+    assert g.count(3, sme.GPU_LIGHT, mem_limit_bytes=8 << 20) == want
+    small_batches = sme.last_stats().batches
+    assert g.count(3, sme.GPU_LIGHT) == want
+    assert sme.last_stats().batches < small_batches
+
+
 def test_edge_cases():
     # empty-ish, single edge, star, path, triangle
     def csr(n, edges):
