@@ -197,7 +197,9 @@ int32_t sme_query_vertex_count(int32_t query_type);
 /* plan_type: 0 TraversalPlan, 1 ReuseTraversalPlan (autogen as test_plan -t 1),
  * 2 LazyTraversalPlan (NON_MATERIALIZE_OPT as test_plan -t 2),
  * 3 ReuseTraversalPlan with the hard-coded plan (patternmatch default),
- * 4 LazyTraversalPlan with compress_level SPECIAL.
+ * 4 LazyTraversalPlan with compress_level SPECIAL,
+ * 5 the level programs the engine runs for algo 4, 5 and 6 (default options),
+ * 6 as 5 for a graph without self loops (the usual case).
  * Writes a NUL-terminated text description; returns SME_ERR_CAPACITY when
  * `cap` is too small (*needed holds the size). */
 sme_status sme_plan_describe(int32_t query_type, int32_t plan_type, char* buf,

@@ -71,7 +71,7 @@ struct RunOut {
 static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t* host_out, uint64_t cap) {
   CheckOpts(o);
   auto t0 = std::chrono::steady_clock::now();
-  Program prog = Compile(o, enumerate);
+  Program prog = Compile(o, enumerate, g->g.LoopFree());
   if (g->g.oriented) RequireOrientable(prog, o.enable_ordering != 0);
   CtxSlot& slot = SlotFor(o.device);
   std::lock_guard<std::mutex> lock(slot.mu);
@@ -366,17 +366,18 @@ sme_status sme_plan_describe(int32_t q, int32_t plan_type, char* buf, uint64_t c
       case 2: text = LazyPlan(query, SME_COMPRESS_NON_MATERIALIZE_OPT).Describe(); break;
       case 3: text = ReusePlan(query, false).Describe(); break;
       case 4: text = LazyPlan(query, SME_COMPRESS_SPECIAL).Describe(); break;
-      case 5: {
+      case 5:
+      case 6: {
         sme_opts o;
         sme_opts_default(&o);
         o.query_type = q;
         for (int a : {SME_GPU_GPSM, SME_GPU_GPSM_REUSE, SME_GPU_LIGHT}) {
           o.algo = a;
-          text += Compile(o, false).Describe();
+          text += Compile(o, false, plan_type == 6).Describe();
         }
         break;
       }
-      default: Fail(SME_ERR_INVALID_ARG, "plan_type must be 0..5");
+      default: Fail(SME_ERR_INVALID_ARG, "plan_type must be 0..6");
     }
   });
   if (st != SME_OK) return st;

@@ -282,7 +282,7 @@ std::vector<int> PlanSetReuse(const LazyPlan& lp, const Query& q, std::vector<in
 // M[w] > M[v] gives x != M[v]): the clique plans fill every unordered pair
 // with NON_EQUAL, yet their total order makes those checks dead.  Steps
 // without `!=` run the intersection without an exclusion array.
-void PruneImpliedExclusions(Program& p) {
+void PruneImpliedExclusions(Program& p, bool loop_free) {
   const int n = p.n;
   std::vector<bool> mat(n, false);
   std::vector<std::vector<StepCond>> cset(n), known(n);
@@ -295,11 +295,18 @@ void PruneImpliedExclusions(Program& p) {
     if (s.kind == S_MATERIALIZE || s.kind == S_FILTER)
       for (const StepCond& c : cset[u])
         if (c.op != NON_EQUAL) strict.push_back(c);
+    // lists the candidates are drawn from (a reused set stands for its lists)
+    const std::vector<uint8_t>& lists = s.full_conn.empty() ? s.conn : s.full_conn;
+    const bool intersects = s.kind == S_COMPUTE || s.kind == S_COMPUTE_COUNT || s.kind == S_PATH_COUNT;
     std::vector<StepCond> kept;
     for (const StepCond& c : s.cond) {
       bool dead = c.op == NON_EQUAL && mat[c.operand] &&
                   (Implies(strict, {StepCond{LESS_THAN, c.operand}}, mat, known) ||
                    Implies(strict, {StepCond{LARGER_THAN, c.operand}}, mat, known));
+      // x in N(M[v]) and no self loop: x != M[v]
+      if (c.op == NON_EQUAL && loop_free && intersects &&
+          std::find(lists.begin(), lists.end(), c.operand) != lists.end())
+        dead = true;
       if (!dead) kept.push_back(c);
     }
     // bookkeeping uses the full condition lists (facts, not checks)
@@ -439,7 +446,7 @@ Program CompileLight(const Query& q, int compress_level, bool enumerate, bool se
 }
 }  // namespace
 
-Program Compile(const sme_opts& o, bool enumerate) {
+Program Compile(const sme_opts& o, bool enumerate, bool loop_free) {
   Query q(o.query_type, o.enable_ordering != 0);
   Program p;
   switch (o.algo) {
@@ -462,7 +469,7 @@ Program Compile(const sme_opts& o, bool enumerate) {
   p.query_type = q.type;
   p.algo = o.algo;
   p.enumerate = enumerate;
-  PruneImpliedExclusions(p);
+  PruneImpliedExclusions(p, loop_free);
   for (auto& s : p.steps) {
     std::ostringstream os;
     os << KindName(s.kind) << "(" << (int)s.u << ")";

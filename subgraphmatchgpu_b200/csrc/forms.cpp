@@ -127,7 +127,7 @@ struct sme_server {
       Result res;
       try {
         const HostGraph& hg = r.attached ? r.attached->g : resident[r.gid]->g;
-        Program prog = Compile(r.opts, false);
+        Program prog = Compile(r.opts, false, hg.LoopFree());
         if (hg.oriented) RequireOrientable(prog, r.opts.enable_ordering != 0);
         DeviceGraph* dg = hg.dev;
         bool temp = false;

@@ -27,7 +27,21 @@ uint64_t HostGraph::MaxDegree() const {
   return d;
 }
 
+bool HostGraph::LoopFree() const {
+  int f = loop_free.load(std::memory_order_relaxed);
+  if (f < 0) {
+    uint64_t loops = 0;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : loops)
+    for (uint64_t u = 0; u < n; ++u)
+      for (uintE j = row_ptrs[u]; j < row_ptrs[u + 1]; ++j) loops += cols[j] == u;
+    f = loops == 0 ? 1 : 0;
+    loop_free.store(f, std::memory_order_relaxed);
+  }
+  return f == 1;
+}
+
 void HostGraph::Adopt(std::vector<uintE>&& r, std::vector<uintV>&& c) {
+  loop_free.store(-1, std::memory_order_relaxed);
   row_store = std::move(r);
   col_store = std::move(c);
   n = row_store.empty() ? 0 : row_store.size() - 1;

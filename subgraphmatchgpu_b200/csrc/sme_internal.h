@@ -3,6 +3,7 @@
 // device engine executes.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -38,6 +39,10 @@ struct HostGraph {
   uintV* cols = nullptr;
   bool borrowed = false;
   bool oriented = false;       // each edge once, towards the higher id
+  // 1 no vertex lists itself, 0 some vertex does, -1 not yet checked
+  // (server workers may ask concurrently: the flag is atomic)
+  mutable std::atomic<int> loop_free{-1};
+  bool LoopFree() const;
   std::vector<uintE> row_store;
   std::vector<uintV> col_store;
   DeviceGraph* dev = nullptr;  // resident device copy (may be null)
@@ -184,7 +189,9 @@ struct Program {
   std::string Describe() const;
 };
 // Builds the level program of a query under one of the three GPU plans.
-Program Compile(const sme_opts& o, bool enumerate);
+// `loop_free`: the graph has no self loop, so a candidate drawn from N(M[v])
+// differs from M[v] without a check.
+Program Compile(const sme_opts& o, bool enumerate, bool loop_free = false);
 // A clique query whose symmetry breaking is the total order u0 < u1 < ...
 bool IsOrderedClique(const Query& q);
 // Fails unless `p` counts correctly on an oriented graph: an ordered clique

@@ -156,6 +156,25 @@ def test_edge_cases():
     assert g.count(0) == 0
 
 
+def test_graph_with_self_loops_keeps_injectivity_checks():
+    # the != checks against list owners are dropped only for loop-free graphs;
+    # with self loops a vertex is in its own list and the checks must stay
+    rp, cl = O.read_bin(golden_graph_path("er_n64_d12"))
+    n = len(rp) - 1
+    adj = [set(cl[rp[u]:rp[u + 1]].tolist()) for u in range(n)]
+    for u in range(0, n, 3):
+        adj[u].add(u)
+    lrp = np.zeros(n + 1, np.uint64)
+    for u in range(n):
+        lrp[u + 1] = lrp[u] + len(adj[u])
+    lcl = np.array([v for u in range(n) for v in sorted(adj[u])], np.uint32)
+    g = sme.Graph.from_csr(lrp, lcl)
+    for q in (0, 1, 2, 3, 4, 7):
+        want = O.count(lrp, lcl, q)
+        for algo in ALGOS:
+            assert g.count(q, algo) == want, (q, algo)
+
+
 def test_resident_graph_and_stats():
     g = sme.Graph.rmat(14, 8, seed=1)
     rp, cl = g.csr()

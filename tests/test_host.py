@@ -225,3 +225,10 @@ def test_light_clique_programs_start_from_earlier_sets():
     q1 = sme.plan_describe(1, 5).split("program Q")[3]
     assert "reuse=" not in q1
     assert "COMPUTE(2) conn=(1) cond=(>0,!=1)" in q1
+    # without self loops a candidate from N(M[v]) differs from M[v]: the
+    # 4-cycle keeps only its order conditions
+    q1 = sme.plan_describe(1, 6).split("program Q")[3]
+    assert "COMPUTE(2) conn=(1) cond=(>0)" in q1
+    assert "COMPUTE_COUNT(3) conn=(0,2) cond=(>0,>1)" in q1
+    # a != against a vertex that is not a list owner stays (house: u4 vs u1)
+    assert "!=" in sme.plan_describe(4, 6).split("program Q")[3]
