@@ -95,8 +95,16 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
   } else {
     DeviceGraph* dg = g->g.dev;
     bool temp = false;
+    const size_t graph_mark = ctx.arena.Mark();
     if (!dg || dg->device != o.device) {
-      dg = UploadGraph(g->g, o.device, ctx.stream, &h2d);
+      // not resident: the graph shares the call's arena (budget covers
+      // frontiers + graph) and leaves with it
+      try {
+        dg = UploadGraphToArena(g->g, ctx, &h2d);
+      } catch (...) {
+        ctx.arena.Release(graph_mark);
+        throw;
+      }
       temp = true;
     }
     uint32_t* d_out = nullptr;
@@ -121,10 +129,12 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
     } catch (...) {
       if (d_out) cudaFree(d_out);
       if (temp) FreeDeviceGraph(dg);
+      ctx.arena.Release(graph_mark);
       throw;
     }
     if (d_out) cudaFree(d_out);
     if (temp) FreeDeviceGraph(dg);
+    ctx.arena.Release(graph_mark);
   }
   r.stats.h2d_bytes = h2d;
   r.stats.d2h_bytes = d2h;

@@ -878,7 +878,10 @@ __global__ void k_build_bitmaps(const uintE* __restrict__ rp, const uint32_t* __
 
 // Bitmaps for the vertices of highest degree (>= kHubMinDegree) within a
 // byte budget (SME_HUB_BITMAP_MB, default 256 MiB); a bitmap is n bits.
-void BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream) {
+// `alloc` hands out device memory (cudaMalloc, or the context's arena for a
+// per-call upload); `scratch_owned` frees the temporary hub list afterwards.
+template <typename Alloc>
+void BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream, Alloc alloc, bool scratch_owned) {
   const uint64_t kHubMinDegree = 256;
   uint64_t budget = 256ULL << 20;
   if (const char* e = std::getenv("SME_HUB_BITMAP_MB")) budget = std::strtoull(e, nullptr, 10) << 20;
@@ -900,17 +903,16 @@ void BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream) {
     hubs[i] = cand[i].second;
     slot[cand[i].second] = (int32_t)i;
   }
-  uint32_t* d_hubs = nullptr;
-  CK(cudaMalloc((void**)&d->hub_slot, g.n * sizeof(int32_t)));
-  CK(cudaMalloc((void**)&d->bitmaps, hubs.size() * (size_t)words * 4));
-  CK(cudaMalloc((void**)&d_hubs, hubs.size() * 4));
+  d->hub_slot = (int32_t*)alloc(g.n * sizeof(int32_t));
+  d->bitmaps = (uint32_t*)alloc(hubs.size() * (size_t)words * 4);
+  uint32_t* d_hubs = (uint32_t*)alloc(hubs.size() * 4);
   CK(cudaMemcpyAsync(d->hub_slot, slot.data(), g.n * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d_hubs, hubs.data(), hubs.size() * 4, cudaMemcpyHostToDevice, stream));
   CK(cudaMemsetAsync(d->bitmaps, 0, hubs.size() * (size_t)words * 4, stream));
   k_build_bitmaps<<<(unsigned)hubs.size(), 256, 0, stream>>>(d->row_ptrs, d->cols, d_hubs, words, d->bitmaps);
   CK(cudaStreamSynchronize(stream));
   CK(cudaGetLastError());
-  cudaFree(d_hubs);
+  if (scratch_owned) cudaFree(d_hubs);
   d->words = words;
   d->nhubs = (uint32_t)hubs.size();
 }
@@ -928,7 +930,12 @@ DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, ui
     CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, stream));
     if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
-    BuildHubBitmaps(d, g, stream);
+    auto dev_alloc = [](size_t bytes) {
+      void* p = nullptr;
+      CK(cudaMalloc(&p, bytes));
+      return p;
+    };
+    BuildHubBitmaps(d, g, stream, dev_alloc, true);
   } catch (...) {
     FreeDeviceGraph(d);
     throw;
@@ -937,8 +944,35 @@ DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, ui
   return d;
 }
 
+DeviceGraph* UploadGraphToArena(const HostGraph& g, DeviceContext& ctx, uint64_t* h2d) {
+  CK(cudaSetDevice(ctx.device));
+  auto* d = new DeviceGraph();
+  d->device = ctx.device;
+  d->n = g.n;
+  d->m = g.m;
+  d->in_arena = true;
+  try {
+    auto arena_alloc = [&ctx](size_t bytes) { return ctx.arena.Alloc(bytes); };
+    d->row_ptrs = (uintE*)arena_alloc((g.n + 1) * sizeof(uintE));
+    d->cols = (uintV*)arena_alloc(std::max<uint64_t>(g.m, 1) * sizeof(uintV));
+    CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, ctx.stream));
+    if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, ctx.stream));
+    BuildHubBitmaps(d, g, ctx.stream, arena_alloc, false);
+    CK(cudaStreamSynchronize(ctx.stream));
+  } catch (...) {
+    delete d;
+    throw;
+  }
+  if (h2d) *h2d += (g.n + 1) * sizeof(uintE) + g.m * sizeof(uintV);
+  return d;
+}
+
 void FreeDeviceGraph(DeviceGraph* d) {
   if (!d) return;
+  if (d->in_arena) {  // released with the arena mark taken before the upload
+    delete d;
+    return;
+  }
   cudaSetDevice(d->device);
   if (d->row_ptrs) cudaFree(d->row_ptrs);
   if (d->cols && !d->host_mapped) cudaFree(d->cols);
@@ -1000,6 +1034,7 @@ class Executor {
     if (stride == 0) stride = 1;
     auto t0 = std::chrono::steady_clock::now();
     size_t mark = A_.Mark();
+    A_.peak = mark;  // high-water mark of this run
     ctrl_ = (unsigned long long*)A_.Alloc(8 * sizeof(unsigned long long));
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));

@@ -14,6 +14,7 @@ struct DeviceGraph {
   uintE* row_ptrs = nullptr;
   uintV* cols = nullptr;
   bool host_mapped = false;  // cols live in mapped pinned host memory (EXT_UMA)
+  bool in_arena = false;     // arrays live in a context's arena (per-call upload)
   // dense adjacency bitmaps of the highest-degree vertices
   int32_t* hub_slot = nullptr;  // per vertex: bitmap slot or -1
   uint32_t* bitmaps = nullptr;  // nhubs x words
@@ -47,6 +48,9 @@ DeviceContext* CreateContext(int device, uint64_t bytes);
 void DestroyContext(DeviceContext* c);
 
 DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, uint64_t* h2d_bytes);
+// Per-call upload into the context's arena: no device allocation; the caller
+// takes an arena mark before and releases it after the run.
+DeviceGraph* UploadGraphToArena(const HostGraph& g, DeviceContext& ctx, uint64_t* h2d_bytes);
 void FreeDeviceGraph(DeviceGraph* d);
 
 struct RunResult {

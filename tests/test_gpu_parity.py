@@ -124,6 +124,18 @@ def test_auto_budget_after_a_small_budget_call(graphs, golden):
     assert sme.last_stats().batches < small_batches
 
 
+def test_failed_upload_releases_the_arena():
+    # a graph that is not resident is uploaded into the call's arena; when it
+    # does not fit, the call fails with OOM and the arena is whole again
+    big = sme.Graph.rmat(16, 16, seed=3)
+    with pytest.raises(sme.SmeError) as e:
+        big.count(3, mem_limit_bytes=4 << 20)
+    assert e.value.status == 3
+    small = sme.Graph.clique(12)
+    for _ in range(3):
+        assert small.count(3, mem_limit_bytes=4 << 20) == 495
+
+
 def test_edge_cases():
     # empty-ish, single edge, star, path, triangle
     def csr(n, edges):
