@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--list-only", action="store_true", help="no hub bitmaps (comparison)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-s22", action="store_true", help="skip the R-MAT s22 4-clique leg")
+    ap.add_argument("--no-l2-flush", action="store_true", help="do not flush L2 between steps")
     return ap.parse_args()
 
 
@@ -407,8 +408,18 @@ def main():
     items = work_items(args, n)
     tune = {"warp_granularity": args.granularity, "list_only": int(args.list_only)}
 
+    # L2 (126 MB) is flushed before every step by writing a 256 MiB buffer, so
+    # no step starts with the previous step's lists in cache
+    flush_buf = None if args.no_l2_flush else torch.empty(64 << 20, dtype=torch.int32, device=f"cuda:{local}")
+
+    def flush_l2():
+        if flush_buf is not None:
+            flush_buf.fill_(1)
+        torch.cuda.synchronize()
+
     def step(i):
         q, a, b, st = items[i % len(items)]
+        flush_l2()
         c = g.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
         return c, sme.last_stats()
 
@@ -453,7 +464,7 @@ def main():
         gh.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
         for i in range(args.steps):
             q, a, b, st = items[(args.warmup + i) % len(items)]
-            torch.cuda.synchronize()
+            flush_l2()
             t0 = time.perf_counter()
             e_inst += gh.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
             e_t += time.perf_counter() - t0
@@ -512,7 +523,9 @@ def main():
                                    f"(Q3 4-clique, Q1 4-cycle, Q2 diamond), plan algo {args.algo} "
                                    f"(6=LIGHT), IN_MEMORY_GPU; tasks: {args.tasks} root ranges per query, "
                                    f"4-cycle {args.q1_tasks} strided tasks of every {args.q1_stride}-th root",
-                       "l2": "inputs larger than L2 (CSR bytes %d)" % (8 * (n + 1) + 4 * m),
+                       "l2": ("L2 flushed before every step (256 MiB write, outside the timed region); "
+                              if not args.no_l2_flush else "no L2 flush; ") +
+                             "CSR bytes %d" % (8 * (n + 1) + 4 * m),
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "per_query": {str(q): {"instances": v[0], "device_ms": v[1],
                                               "phase_ms": dict(zip(sme.Stats.PHASES, [round(x, 3) for x in v[2]]))}

@@ -364,12 +364,13 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
 // lane finds its element's path by binary search over the 32 range offsets.
 // Sets stay sorted and compact per path: the rank of an element is its path's
 // running count plus the valid lanes before it in the same path segment.
+template <int NLM, int NEX>
 struct FlatPath {
-  const uint32_t* L[MAXV];  // L[0] = pivot (already offset by r0)
-  const uint32_t* B[MAXV];  // hub bitmaps (null: binary search)
-  uint32_t N[MAXV];
-  uint32_t ne[MAXV];
-  const uint32_t* W;        // ranked-count partner set
+  const uint32_t* L[NLM];  // L[0] = pivot (already offset by r0); others cut to the pivot's value range
+  const uint32_t* B[NLM];  // hub bitmaps (null: binary search)
+  uint32_t N[NLM];
+  uint32_t ne[NEX > 0 ? NEX : 1];
+  const uint32_t* W;       // ranked-count partner set
   uint32_t WN;
   uint64_t out_off;
   uint32_t written;
@@ -377,13 +378,15 @@ struct FlatPath {
 };
 constexpr int FLAT_WARPS = WARP_BLOCK / 32;
 
-template <int MODE>
-__global__ void __launch_bounds__(WARP_BLOCK) k_compute_flat(
+// Specialised like k_compute: NLM bounds the intersected lists, NEX = 0 for
+// steps without `!=` conditions (the launcher guarantees both).
+template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV>
+__global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute_flat(
     DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
     uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
   const uintE* __restrict__ rp = G.rp;
   const uint32_t* __restrict__ cols = G.cols;
-  __shared__ FlatPath sp[FLAT_WARPS][32];
+  __shared__ FlatPath<NLM, NEX> sp[FLAT_WARPS][32];
   __shared__ uint32_t soff[FLAT_WARPS][33];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -395,13 +398,13 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute_flat(
     uint32_t len = 0;
     bool view = false;
     if (p < F.P) {
-      FlatPath& fp = sp[wl][lane];
-      const uint32_t* L[MAXV];
-      const uint32_t* B[MAXV];
-      uint32_t N[MAXV];
+      FlatPath<NLM, NEX>& fp = sp[wl][lane];
+      const uint32_t* L[NLM];
+      const uint32_t* B[NLM];
+      uint32_t N[NLM];
       int nl = 0;
 #pragma unroll
-      for (int i = 0; i < MAXV; ++i) {
+      for (int i = 0; i < NLM; ++i) {
         B[i] = nullptr;
         if (i < s.nconn) {
           uint32_t v = F.inst[s.conn[i]][p];
@@ -414,16 +417,16 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute_flat(
       }
       if (s.reuse >= 0) {
 #pragma unroll
-        for (int i = 0; i < MAXV; ++i)
+        for (int i = 0; i < NLM; ++i)
           if (i == nl) GetSet(F, s.reuse, p, L[i], N[i]);
         ++nl;
       }
       uint64_t b = 12ULL * s.nconn;
 #pragma unroll
-      for (int i = 0; i < MAXV; ++i)
+      for (int i = 0; i < NLM; ++i)
         if (i < nl) b += 4ULL * N[i];
 #pragma unroll
-      for (int i = 1; i < MAXV; ++i) {
+      for (int i = 1; i < NLM; ++i) {
         if (i < nl && N[i] < N[0]) {
           const uint32_t* tp = L[0];
           L[0] = L[i];
@@ -436,7 +439,7 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute_flat(
           N[i] = tn;
         }
       }
-      Bounds bd = MakeBounds(s.cond, F, p);
+      BoundsT<NEX> bd = MakeBounds<NEX>(s.cond, F, p);
       uint32_t r0 = 0, r1 = 0;
       if (nl > 0) Range(L[0], N[0], bd, r0, r1);
       if (MODE == 0) {
@@ -457,14 +460,22 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute_flat(
       if (MODE == 1 && s.with_u >= 0) GetSet(F, s.with_u, p, fp.W, fp.WN);
       fp.L[0] = L[0] + r0;
       fp.N[0] = r1 - r0;
+      // the other lists only matter between the pivot's first and last value
+      const uint32_t lo_v = r1 > r0 ? __ldg(L[0] + r0) : 0, hi_v = r1 > r0 ? __ldg(L[0] + r1 - 1) : 0;
 #pragma unroll
-      for (int i = 1; i < MAXV; ++i) {
+      for (int i = 1; i < NLM; ++i) {
+        fp.B[i] = B[i];
         fp.L[i] = L[i];
         fp.N[i] = N[i];
-        fp.B[i] = B[i];
+        if (i < nl && !B[i] && r1 > r0) {
+          const uint32_t a = LowerBound(L[i], N[i], lo_v);
+          const uint32_t e = a + LowerBound(L[i] + a, N[i] - a, hi_v + 1);
+          fp.L[i] = L[i] + a;
+          fp.N[i] = e - a;
+        }
       }
 #pragma unroll
-      for (int i = 0; i < MAXV; ++i) fp.ne[i] = bd.ne[i];
+      for (int i = 0; i < NEX; ++i) fp.ne[i] = bd.ne[i];
       fp.nne = (uint8_t)bd.nne;
       fp.nl = (uint8_t)nl;
       fp.written = 0;
@@ -495,15 +506,16 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute_flat(
         }
         j = lo;
       }
-      const FlatPath& fp = sp[wl][j];
+      const FlatPath<NLM, NEX>& fp = sp[wl][j];
       bool ok = in;
       uint32_t v = 0;
       if (ok) {
         v = __ldg(fp.L[0] + (f - soff[wl][j]));
-        for (int k = 0; k < fp.nne; ++k)
-          if (v == fp.ne[k]) ok = false;
 #pragma unroll
-        for (int q = 1; q < MAXV; ++q) {
+        for (int k = 0; k < NEX; ++k)
+          if (k < fp.nne && v == fp.ne[k]) ok = false;
+#pragma unroll
+        for (int q = 1; q < NLM; ++q) {
           if (q < fp.nl && ok) {
             if (fp.B[q]) {
               ok = BitTest(fp.B[q], v);
@@ -541,7 +553,7 @@ __global__ void __launch_bounds__(WARP_BLOCK) k_compute_flat(
       (void)valid;
     }
     if (MODE != 1 && p < F.P && !view) {  // views were published above
-      const FlatPath& fp = sp[wl][lane];
+      const FlatPath<NLM, NEX>& fp = sp[wl][lane];
       out_ptr[p] = MODE == 0 ? (uint64_t)(out_data + fp.out_off) : 0;
       out_cnt[p] = fp.written;
       if (MODE == 0) bytes += 4ULL * fp.written;
@@ -1182,6 +1194,19 @@ class Executor {
                                                                           acc, err);
   }
 
+  template <int MODE, int MINB, int NLM>
+  void LaunchFlat(bool ne, const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est, uint32_t b0,
+                  uint64_t* ptr, uint32_t* cnt, uint32_t* data, uint64_t cap, unsigned long long* acc,
+                  uint32_t* err) {
+    const unsigned grid = WarpGrid((F.P + 31) / 32);
+    if (ne)
+      k_compute_flat<MODE, MINB, NLM, MAXV><<<grid, WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap,
+                                                                         acc, err);
+    else
+      k_compute_flat<MODE, MINB, NLM, 0><<<grid, WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc,
+                                                                      err);
+  }
+
   // Intersection launch: warp per path, specialised (granularity 0 auto, 3),
   // warp per path generic (1) or flattened over 32 paths per warp (2).
   template <int MODE>
@@ -1209,11 +1234,20 @@ class Executor {
               : LaunchWarp<MODE, 6, 3>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
       else
         LaunchWarp<MODE, 6, MAXV>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
-    } else if (gran == 1)
+    } else if (gran == 1) {
       k_compute<MODE><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
-    else
-      k_compute_flat<MODE><<<WarpGrid((F.P + 31) / 32), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data,
-                                                                              cap, acc, err);
+    } else {
+      // flattened, specialised the same way
+      const int nl = ds.nconn + (ds.reuse >= 0 ? 1 : 0);
+      bool ne = false;
+      for (int i = 0; i < ds.cond.n; ++i) ne |= ds.cond.op[i] == 2;
+      if (nl <= 2)
+        LaunchFlat<MODE, 8, 2>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+      else if (nl <= 3)
+        LaunchFlat<MODE, 6, 3>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+      else
+        LaunchFlat<MODE, 4, MAXV>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+    }
     TimerStop(t, MODE == 0 ? kPhaseCompute : MODE == 1 ? kPhaseComputeCount : kPhasePathCount);
     Launched();
   }

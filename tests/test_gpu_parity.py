@@ -34,7 +34,7 @@ def test_counts_match_reference_on_golden_graphs(graphs, golden, algo):
 
 @pytest.mark.parametrize("gran", [1, 2, 3])
 def test_intersection_granularities(graphs, golden, gran):
-    # 1: warp per path generic, 2: flattened over 32 paths per warp,
+    # 1: warp per path generic, 2: flattened over 32 paths per warp (specialised),
     # 3: specialised warp per path at six blocks per SM (0, auto, runs in
     # every other test)
     for name in ("rmat_s12_ef8", "ba_n600_m4", "k12"):
