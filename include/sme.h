@@ -190,6 +190,30 @@ sme_status sme_enumerate(sme_graph* g, const sme_opts* opts, uint32_t* out,
                          uint64_t cap_instances, uint64_t* n_out);
 /* Stats of the last sme_count/sme_enumerate issued by this thread. */
 sme_status sme_last_stats(sme_stats* stats);
+
+/* ---- partitioned graphs (HYBRID_CPU_GPU, -m 0 -e FILE -p P) ------------- */
+/* GraphIO::ReadPartitionFile (src/graph/GraphIO.h:66-86): n partition ids,
+ * one per vertex, whitespace separated, into vertex_partition[n].
+ * partition_num == 1 or an empty path puts every vertex in partition 0.
+ * A short file, an id >= partition_num or a largest id other than
+ * partition_num - 1 (an assert in the reference) return SME_ERR_BAD_FILE. */
+sme_status sme_read_partition_file(const char* path, uint64_t n, uint32_t partition_num,
+                                   uint32_t* vertex_partition);
+/* The subgraph induced by partition p, its vertices renumbered in ascending
+ * global id (GraphPartition::BuildIntraPartition,
+ * src/graph/GraphPartition.h:36-95). */
+sme_status sme_graph_partition(const sme_graph* g, const uint32_t* vertex_partition, uint32_t p,
+                               sme_graph** out);
+/* The counts of -m 0 (HybridSeparatePatternMatch / Interplay / Coprocess,
+ * src/gpu/executor/): *total over the whole graph, intra[p] (may be NULL)
+ * the instances inside partition p; the inter-partition count is
+ * total - sum(intra).  algo 5 or 6 as the reference allows for this mode;
+ * execute_mode 0 or 1.  The whole graph runs in one in-memory pass on the
+ * GPU (it fits in HBM), so the CPU/GPU work split of variants O0-O3 is not
+ * reproduced; the counts are the same. */
+sme_status sme_count_partitioned(sme_graph* g, const sme_opts* opts, const uint32_t* vertex_partition,
+                                 uint32_t partition_num, uint64_t* total, uint64_t* intra);
+
 /* Number of pattern vertices of query q (Query.h:84-434). */
 int32_t sme_query_vertex_count(int32_t query_type);
 

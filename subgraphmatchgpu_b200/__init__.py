@@ -101,6 +101,10 @@ SIGNATURES = {
     "sme_graph_preprocess": (C.c_int, [_P]),
     "sme_graph_validate": (C.c_int, [_P]),
     "sme_graph_degree_order": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_void_p), C.c_void_p]),
+    "sme_read_partition_file": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint32, C.c_void_p]),
+    "sme_graph_partition": (C.c_int, [_P, C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "sme_count_partitioned": (C.c_int, [_P, C.POINTER(Opts), C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64),
+                                        C.c_void_p]),
     "sme_graph_is_oriented": (C.c_int32, [_P]),
     "sme_graph_to_device": (C.c_int, [_P, C.c_int]),
     "sme_graph_release_device": (C.c_int, [_P]),
@@ -278,6 +282,24 @@ class Graph:
     def oriented(self) -> bool:
         return bool(lib().sme_graph_is_oriented(self._h))
 
+    def partition(self, vertex_partition, p: int) -> "Graph":
+        """Subgraph induced by partition p (ascending global ids)."""
+        vp = np.ascontiguousarray(vertex_partition, dtype=np.uint32)
+        h = C.c_void_p()
+        _check(lib().sme_graph_partition(self._h, vp.ctypes.data, p, C.byref(h)))
+        return Graph(h.value)
+
+    def count_partitioned(self, query: int, vertex_partition, partition_num: int, algo: int = GPU_LIGHT, **kw):
+        """-m 0: (total, intra-partition counts per partition)."""
+        vp = np.ascontiguousarray(vertex_partition, dtype=np.uint32)
+        o = opts(query, algo, 0, **kw)
+        total = C.c_uint64()
+        intra = np.zeros(partition_num, np.uint64)
+        _check(lib().sme_count_partitioned(self._h, C.byref(o), vp.ctypes.data, partition_num, C.byref(total),
+                                           intra.ctypes.data))
+        return total.value, intra
+
+
     def to_device(self, device: int = 0) -> None:
         _check(lib().sme_graph_to_device(self._h, device))
 
@@ -414,5 +436,13 @@ class Server:
 __all__ = [
     "BatchPlan", "Server",
     "Graph", "SmeError", "Opts", "Stats", "lib", "opts", "plan_describe", "last_stats", "query_vertex_count",
+    "read_partition_file",
     "GPU_GPSM", "GPU_GPSM_REUSE", "GPU_LIGHT", "IN_MEMORY_GPU", "EXTERNAL_GPU", "SIGNATURES", "QUERY_NAMES",
 ]
+
+
+def read_partition_file(path: str, n: int, partition_num: int) -> np.ndarray:
+    """GraphIO::ReadPartitionFile: uint32 partition id per vertex."""
+    out = np.zeros(max(n, 1), np.uint32)
+    _check(lib().sme_read_partition_file(path.encode(), n, partition_num, out.ctypes.data))
+    return out[:n]

@@ -341,6 +341,67 @@ sme_status sme_count(sme_graph* g, const sme_opts* opts, uint64_t* count) {
   return Guard([&] { *count = Execute(g, *opts, false, nullptr, 0).count; });
 }
 
+sme_status sme_read_partition_file(const char* path, uint64_t n, uint32_t partition_num, uint32_t* vertex_partition) {
+  if (!vertex_partition && n) return SME_ERR_INVALID_ARG;
+  return Guard([&] { ReadPartitionFile(path ? path : "", n, partition_num, vertex_partition); });
+}
+
+sme_status sme_graph_partition(const sme_graph* g, const uint32_t* vertex_partition, uint32_t p, sme_graph** out) {
+  if (!g || !vertex_partition || !out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    std::unique_ptr<sme_graph> r(new sme_graph());
+    InducedPartition(g->g, vertex_partition, p, r->g, nullptr);
+    *out = r.release();
+  });
+}
+
+// HYBRID_CPU_GPU (-m 0): the whole graph fits in one B200's memory, so the
+// total is counted on it in one in-memory run, and each partition's
+// intra-partition share on its induced subgraph; the inter-partition share
+// is the difference.  Plans as InitGPUInstance allows for this mode
+// (src/gpu/PatternMatchGPUInstance.cuh:43-63): reuse BFS or LIGHT.
+sme_status sme_count_partitioned(sme_graph* g, const sme_opts* opts, const uint32_t* vertex_partition,
+                                 uint32_t partition_num, uint64_t* total, uint64_t* intra) {
+  if (!g || !opts || !vertex_partition || !total || partition_num == 0) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    if (opts->algo != SME_GPU_GPSM_REUSE && opts->algo != SME_GPU_LIGHT)
+      Fail(SME_ERR_INVALID_ARG, "HYBRID_CPU_GPU runs the reuse BFS (5) or LIGHT (6) plan");
+    if (opts->execute_mode != SME_HYBRID_CPU_GPU && opts->execute_mode != SME_IN_MEMORY_GPU)
+      Fail(SME_ERR_INVALID_ARG, "partitioned counting takes execute_mode 0 (HYBRID_CPU_GPU) or 1");
+    for (uint64_t u = 0; u < g->g.n; ++u)
+      if (vertex_partition[u] >= partition_num)
+        Fail(SME_ERR_INVALID_ARG, "vertex " + std::to_string(u) + " has partition id " +
+                                      std::to_string(vertex_partition[u]) + " >= partition_num");
+    sme_opts o = *opts;
+    o.execute_mode = SME_IN_MEMORY_GPU;
+    o.root_begin = o.root_end = 0;
+    o.root_stride = 1;
+    double elapsed = 0;
+    uint64_t launches = 0, h2d = 0;
+    *total = Execute(g, o, false, nullptr, 0).count;
+    elapsed += t_last_stats.elapsed_ms;
+    launches += t_last_stats.kernel_launches;
+    h2d += t_last_stats.h2d_bytes;
+    uint64_t intra_sum = 0;
+    for (uint32_t p = 0; p < partition_num; ++p) {
+      sme_graph part;
+      InducedPartition(g->g, vertex_partition, p, part.g, nullptr);
+      const uint64_t c = part.g.n ? Execute(&part, o, false, nullptr, 0).count : 0;
+      if (part.g.n) {
+        elapsed += t_last_stats.elapsed_ms;
+        launches += t_last_stats.kernel_launches;
+        h2d += t_last_stats.h2d_bytes;
+      }
+      if (intra) intra[p] = c;
+      intra_sum += c;
+    }
+    if (intra_sum > *total) Fail(SME_ERR_CUDA, "intra-partition counts exceed the total");
+    t_last_stats.elapsed_ms = elapsed;
+    t_last_stats.kernel_launches = launches;
+    t_last_stats.h2d_bytes = h2d;
+  });
+}
+
 sme_status sme_enumerate(sme_graph* g, const sme_opts* opts, uint32_t* out, uint64_t cap, uint64_t* n_out) {
   if (!g || !opts || !n_out || (cap && !out)) return SME_ERR_INVALID_ARG;
   sme_status st = Guard([&] {

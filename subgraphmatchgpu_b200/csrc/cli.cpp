@@ -42,7 +42,8 @@ void Help() {
                "Q4 (house) 4, Q5 (quad triangle) 5, Q6 (near5clique) 6, Q7 (5 clique) 7, "
                "Q8 (chordal roof) 8, Q9 (three triangle) 9, Q10 (solar square) 10, Q11 (6 clique) 11, "
                "Q12 (near near 5 clique) 12, Q13 (triangle in diamond) 13\n";
-  std::cout << "MODE: HYBRID_CPU_GPU=0 (not supported), IN_MEMORY_GPU=1, EXTERNAL_GPU=2\n";
+  std::cout << "MODE: HYBRID_CPU_GPU=0 (partition counts; -e PARTITION_FILENAME -p PARTITION_NUM), "
+               "IN_MEMORY_GPU=1, EXTERNAL_GPU=2\n";
   std::cout << "LAZY_TRAVERSAL_COMPRESS_LEVEL: COMPRESS_LEVEL_MATERIALIZE=0, "
                "COMPRESS_LEVEL_NON_MATERIALIZE=1, COMPRESS_LEVEL_NON_MATERIALIZE_OPT=2, "
                "COMPRESS_LEVEL_SPECIAL(DEFAULT)=3\n";
@@ -90,8 +91,12 @@ int main(int argc, char** argv) {
             << ",lazy_traversal_compress_level=" << o.compress_level
             << ",enable_ordering=" << o.enable_ordering << ",gpu_light_ext_variant=" << o.ext_variant
             << std::endl;
-  if (partition_num != 1) {
-    std::cerr << "partitioned (hybrid) execution is not part of this engine; use -p 1" << std::endl;
+  if (partition_num < 1) {
+    std::cerr << "-p must be >= 1" << std::endl;
+    return 1;
+  }
+  if (partition_num != 1 && o.execute_mode != SME_HYBRID_CPU_GPU) {
+    std::cerr << "-p > 1 partitions the graph for -m 0 (HYBRID_CPU_GPU) only" << std::endl;
     return 1;
   }
   if (dev_num != 1) std::cout << "note: running on device 0 only (-v " << dev_num << " requested)" << std::endl;
@@ -114,7 +119,26 @@ int main(int argc, char** argv) {
   std::cout << "vertex_count=" << n << ",edge_count=" << m << ",max_degree=" << dmax << std::endl;
 
   uint64_t count = 0;
-  if (materialize) {
+  if (o.execute_mode == SME_HYBRID_CPU_GPU) {
+    // -m 0: intra-partition counts per partition of the -e file, the rest is
+    // inter-partition; the total is the answer
+    if (materialize) {
+      std::cerr << "-l 1 runs in -m 1 (IN_MEMORY_GPU)" << std::endl;
+      return 1;
+    }
+    std::vector<uint32_t> part(n ? n : 1);
+    st = sme_read_partition_file(a.Str("-e", "").c_str(), n, (uint32_t)partition_num, part.data());
+    if (st != SME_OK) return Die("partition file", st);
+    std::vector<uint64_t> intra(partition_num);
+    st = sme_count_partitioned(g, &o, part.data(), (uint32_t)partition_num, &count, intra.data());
+    if (st != SME_OK) return Die("count", st);
+    uint64_t intra_sum = 0;
+    for (int p = 0; p < partition_num; ++p) {
+      std::cout << "partition_id=" << p << ",intra_partition_count=" << intra[p] << std::endl;
+      intra_sum += intra[p];
+    }
+    std::cout << "inter_partition_count=" << count - intra_sum << std::endl;
+  } else if (materialize) {
     // enumerate into a host buffer sized by a first counting pass
     st = sme_count(g, &o, &count);
     if (st != SME_OK) return Die("count", st);

@@ -246,6 +246,70 @@ void DegreeOrder(const HostGraph& in, bool orient, HostGraph& out, std::vector<u
   if (new_to_old) *new_to_old = std::move(old_of);
 }
 
+// GraphIO::ReadPartitionFile (src/graph/GraphIO.h:66-86): one partition id
+// per vertex, whitespace separated; a single partition or no file puts every
+// vertex in partition 0.  The reference asserts that the largest id is
+// partition_num - 1; here that, a short file and an id out of range are
+// errors.
+void ReadPartitionFile(const std::string& path, uint64_t n, uint32_t partition_num, uint32_t* map) {
+  if (partition_num == 0) Fail(SME_ERR_INVALID_ARG, "partition_num must be >= 1");
+  if (partition_num == 1 || path.empty()) {
+    std::fill(map, map + n, 0u);
+    return;
+  }
+  std::ifstream in(path);
+  if (!in) Fail(SME_ERR_BAD_FILE, "cannot open partition file " + path);
+  uint64_t max_pid = 0;
+  for (uint64_t u = 0; u < n; ++u) {
+    unsigned long long pid;
+    if (!(in >> pid)) Fail(SME_ERR_BAD_FILE, "partition file " + path + " ends after " + std::to_string(u) +
+                                                 " of " + std::to_string(n) + " vertices");
+    if (pid >= partition_num)
+      Fail(SME_ERR_BAD_FILE, "partition id " + std::to_string(pid) + " of vertex " + std::to_string(u) +
+                                 " is not below partition_num " + std::to_string(partition_num));
+    map[u] = (uint32_t)pid;
+    max_pid = std::max<uint64_t>(max_pid, pid);
+  }
+  if (max_pid + 1 != partition_num)
+    Fail(SME_ERR_BAD_FILE, "partition file " + path + " has " + std::to_string(max_pid + 1) +
+                               " partitions, partition_num is " + std::to_string(partition_num));
+}
+
+// The subgraph induced by the vertices of partition `p`, renumbered in
+// ascending global id so lists stay sorted and the symmetry-breaking order is
+// the global one (GraphPartition::BuildIntraPartition,
+// src/graph/GraphPartition.h:36-95).
+void InducedPartition(const HostGraph& g, const uint32_t* map, uint32_t p, HostGraph& out,
+                      std::vector<uintV>* local_to_global) {
+  const uint64_t n = g.n;
+  std::vector<uintV> local(n, (uintV)-1), global;
+  for (uint64_t u = 0; u < n; ++u)
+    if (map[u] == p) {
+      local[u] = (uintV)global.size();
+      global.push_back((uintV)u);
+    }
+  const uint64_t k = global.size();
+  std::vector<uintE> r(k + 1, 0);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (uint64_t i = 0; i < k; ++i) {
+    const uintV u = global[i];
+    uintE c = 0;
+    for (uintE j = g.row_ptrs[u]; j < g.row_ptrs[u + 1]; ++j) c += map[g.cols[j]] == p;
+    r[i + 1] = c;
+  }
+  for (uint64_t i = 0; i < k; ++i) r[i + 1] += r[i];
+  std::vector<uintV> c(r[k]);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (uint64_t i = 0; i < k; ++i) {
+    const uintV u = global[i];
+    uintE o = r[i];
+    for (uintE j = g.row_ptrs[u]; j < g.row_ptrs[u + 1]; ++j)
+      if (map[g.cols[j]] == p) c[o++] = local[g.cols[j]];
+  }
+  out.Adopt(std::move(r), std::move(c));
+  if (local_to_global) *local_to_global = std::move(global);
+}
+
 void BuildFromEdges(uint64_t n, std::vector<std::pair<uintV, uintV>>& edges, HostGraph& g) {
   std::vector<uintE> r(n + 1, 0);
   for (auto& p : edges) {

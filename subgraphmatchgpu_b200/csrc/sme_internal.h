@@ -59,6 +59,11 @@ void Validate(const HostGraph& g);
 // then applies Preprocess().
 void BuildFromEdges(uint64_t n, std::vector<std::pair<uintV, uintV>>& edges,
                     HostGraph& g);
+// Partition map of n vertices from a partition file (GraphIO::ReadPartitionFile).
+void ReadPartitionFile(const std::string& path, uint64_t n, uint32_t partition_num, uint32_t* map);
+// Subgraph induced by partition p, ascending global ids (GraphPartition).
+void InducedPartition(const HostGraph& g, const uint32_t* map, uint32_t p, HostGraph& out,
+                      std::vector<uintV>* local_to_global);
 // Degree-ordered copy (vertices renumbered by (degree, id) ascending),
 // optionally oriented towards the higher id; new_to_old[new] = old id.
 void DegreeOrder(const HostGraph& in, bool orient, HostGraph& out, std::vector<uintV>* new_to_old);

@@ -24,7 +24,7 @@ def test_help_without_arguments():
 def test_rejects_partitioned_and_bad_degree_order():
     g = golden_graph_path("k12")
     r = run("-f", g, "-d", 0, "-a", 6, "-q", 3, "-m", 1, "-p", 2)
-    assert r.returncode == 1 and "-p 1" in r.stderr
+    assert r.returncode == 1 and "-m 0" in r.stderr
     r = run("-f", g, "-d", 0, "-a", 6, "-q", 3, "-m", 1, "-O", 5)
     assert r.returncode == 1 and "-O" in r.stderr
 
@@ -44,3 +44,30 @@ def test_result_line_matches_reference_count(golden, order):
         assert r.returncode == 0, r.stderr
         m = re.search(r"^total_match_count=(\d+), elapsed_time=([0-9.e+-]+)ms$", r.stdout, re.M)
         assert m and int(m.group(1)) == golden[name]["counts"][str(q)], r.stdout
+
+
+def test_hybrid_mode_checks_the_partition_file(tmp_path):
+    g = golden_graph_path("k12")
+    short = tmp_path / "short.part.2"
+    short.write_text("0\n1\n0\n")
+    r = run("-f", g, "-d", 0, "-a", 6, "-q", 3, "-m", 0, "-e", short, "-p", 2)
+    assert r.returncode == 1 and "partition file" in r.stderr and "ends after 3 of 12" in r.stderr
+    # the reference runs -m 0 with the reuse BFS or LIGHT plan only
+    ok = tmp_path / "k12.part.2"
+    ok.write_text("\n".join(str(i % 2) for i in range(12)))
+    r = run("-f", g, "-d", 0, "-a", 4, "-q", 3, "-m", 0, "-e", ok, "-p", 2)
+    assert r.returncode == 1 and "reuse BFS (5) or LIGHT (6)" in r.stderr
+
+
+@pytest.mark.gpu
+def test_hybrid_mode_result_lines(golden, tmp_path):
+    name = "rmat_s10_ef8"
+    n = 797
+    part = tmp_path / "g.part.3"
+    part.write_text("\n".join(str((i * 7) % 3) for i in range(n)))
+    r = run("-f", golden_graph_path(name), "-d", 0, "-a", 6, "-q", 3, "-m", 0, "-e", part, "-p", 3)
+    assert r.returncode == 0, r.stderr
+    intra = [int(x) for x in re.findall(r"^partition_id=\d+,intra_partition_count=(\d+)$", r.stdout, re.M)]
+    inter = int(re.search(r"^inter_partition_count=(\d+)$", r.stdout, re.M).group(1))
+    total = int(re.search(r"^total_match_count=(\d+), elapsed_time=", r.stdout, re.M).group(1))
+    assert len(intra) == 3 and total == golden[name]["counts"]["3"] and sum(intra) + inter == total

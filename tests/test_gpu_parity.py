@@ -136,6 +136,21 @@ def test_failed_upload_releases_the_arena():
         assert small.count(3, mem_limit_bytes=4 << 20) == 495
 
 
+@pytest.mark.parametrize("algo", [sme.GPU_GPSM_REUSE, sme.GPU_LIGHT])
+def test_partitioned_counts(graphs, golden, algo):
+    # -m 0: the total over the graph, and per partition the instances inside it
+    name = "rmat_s12_ef8"
+    g = graphs[name]
+    n = g.n
+    part = (np.arange(n) * 7 % 4).astype(np.uint32)
+    for q in (0, 3, 4):
+        total, intra = g.count_partitioned(q, part, 4, algo=algo)
+        assert total == golden[name]["counts"][str(q)]
+        for p in range(4):
+            assert intra[p] == O.count(*g.partition(part, p).csr(), q), (q, p)
+        assert intra.sum() <= total
+
+
 def test_edge_cases():
     # empty-ish, single edge, star, path, triangle
     def csr(n, edges):

@@ -232,3 +232,41 @@ def test_light_clique_programs_start_from_earlier_sets():
     assert "COMPUTE_COUNT(3) conn=(0,2) cond=(>0,>1)" in q1
     # a != against a vertex that is not a list owner stays (house: u4 vs u1)
     assert "!=" in sme.plan_describe(4, 6).split("program Q")[3]
+
+
+def test_partition_file_reader(tmp_path):
+    f = tmp_path / "g.part.3"
+    f.write_text("0 1 2\n2 1\n0\n")
+    assert sme.read_partition_file(str(f), 6, 3).tolist() == [0, 1, 2, 2, 1, 0]
+    # one partition (or no file): everything in partition 0
+    assert sme.read_partition_file("", 4, 1).tolist() == [0, 0, 0, 0]
+    for text, n, k in (("0 1\n", 3, 2), ("0 3 1\n", 3, 3), ("0 1 1\n", 3, 3)):
+        f.write_text(text)
+        with pytest.raises(sme.SmeError) as e:
+            sme.read_partition_file(str(f), n, k)
+        assert e.value.status == 2, text
+
+
+def test_induced_partition_subgraph():
+    import oracle_py as O
+    g = sme.Graph.rmat(10, 8, seed=9)
+    rp, cl = g.csr()
+    n = len(rp) - 1
+    part = (np.arange(n) * 5 % 3).astype(np.uint32)
+    for p in range(3):
+        sub = g.partition(part, p)
+        srp, scl = sub.csr()
+        members = np.flatnonzero(part == p)
+        local = {int(v): i for i, v in enumerate(members)}
+        want_edges = sorted((local[int(u)], local[int(v)]) for u in members
+                            for v in cl[rp[u]:rp[u + 1]] if part[v] == p)
+        got_edges = sorted(zip(np.repeat(np.arange(len(srp) - 1), np.diff(srp).astype(np.int64)).tolist(),
+                               scl.tolist()))
+        assert len(srp) - 1 == len(members) and got_edges == want_edges
+        # the induced subgraph keeps exactly the instances inside the partition
+        inst = O.enumerate_sorted(rp, cl, 3)
+        inside = int(np.all(part[inst] == p, axis=1).sum())
+        assert O.count(srp, scl, 3) == inside
+    with pytest.raises(sme.SmeError) as e:
+        g.count_partitioned(3, part, 3, algo=sme.GPU_GPSM)
+    assert e.value.status == 1
