@@ -31,7 +31,10 @@ bool HostGraph::LoopFree() const {
   int f = loop_free.load(std::memory_order_relaxed);
   if (f < 0) {
     uint64_t loops = 0;
-#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : loops)
+    // a thread team only for large graphs: server workers call this for
+    // every attached graph, and teams spawned from several workers at once
+    // oversubscribe the host
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : loops) if (m > (1ULL << 22))
     for (uint64_t u = 0; u < n; ++u)
       for (uintE j = row_ptrs[u]; j < row_ptrs[u + 1]; ++j) loops += cols[j] == u;
     f = loops == 0 ? 1 : 0;
