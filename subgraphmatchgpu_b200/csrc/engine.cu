@@ -1040,7 +1040,6 @@ class Executor {
   // src/gpu/graph/GraphDevTracker.cuh:12-79).
   void SetExternal(const uint32_t* host_cols) { ext_cols_ = host_cols; }
   uint64_t ext_h2d_bytes() const { return ext_bytes_; }
-  uint64_t ext_loads() const { return ext_loads_; }
 
   RunResult Run(uint64_t rb, uint64_t re, uint32_t stride = 1) {
     if (stride == 0) stride = 1;
@@ -1125,7 +1124,7 @@ class Executor {
   unsigned long long* ctrl_ = nullptr;  // [0] count [1] bytes [2] emitted [3] error flags
   uint64_t launches_ = 0, batches_ = 0, paths_ = 0, hot_ = 0;
   const uint32_t* ext_cols_ = nullptr;
-  uint64_t ext_bytes_ = 0, ext_loads_ = 0;
+  uint64_t ext_bytes_ = 0;
 
   // Loads, for the paths of Fb, the adjacency lists step `ds` intersects into
   // a device subgraph allocated in the current arena frame (it stays valid
@@ -1167,7 +1166,6 @@ class Executor {
                                                          sub_cols);
     launches_ += 3;
     ext_bytes_ += sub_m * 4;
-    ++ext_loads_;
     TimerStop(tl, kPhaseExternal);
     (void)mark;
     return DGraph{sub_rp, sub_cols, nullptr, nullptr, 0};

@@ -64,8 +64,9 @@ struct RunResult {
 RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx,
                      uint64_t root_begin, uint64_t root_end, uint32_t* d_out, uint64_t cap,
                      int tuning, uint32_t root_stride = 1);
-// `tuning`: low byte = intersection granularity (0 auto, 1 warp per path,
-// 2 flattened); bit 8 set = no hub bitmaps.
+// `tuning`: low byte = intersection launch (0 auto: warp per path,
+// specialised; 1 warp per path generic; 2 flattened, specialised; 3 as 0 at
+// six blocks per SM); bit 8 set = no hub bitmaps.
 inline int Tuning(const sme_opts& o) { return (o.warp_granularity & 0xff) | (o.list_only ? 0x100 : 0); }
 
 // External (chunked) execution over a graph that stays in host memory.
