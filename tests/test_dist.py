@@ -50,3 +50,21 @@ def test_single_process_is_identity():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.reduce_over_ranks(12.5, 7, None, "cpu") == (12.5, 7.0)
+
+
+def test_reference_arm_prints_the_contract_line():
+    # the CPU arm of the bench, on a small graph: one JSON line with the keys
+    # the driver reads
+    import json
+    import subprocess
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--scale", "10", "--edge-factor", "8"],
+                       capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] in ("port", "reference") and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]

@@ -270,3 +270,26 @@ def test_induced_partition_subgraph():
     with pytest.raises(sme.SmeError) as e:
         g.count_partitioned(3, part, 3, algo=sme.GPU_GPSM)
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("plan_type", [5, 6])
+def test_reused_sets_are_live_where_they_are_read(plan_type):
+    # every step that starts from an earlier candidate set must find that set
+    # among the live sets left by the step before it, and every list it
+    # reads must belong to a vertex materialised by then
+    step_re = re.compile(r"^(\d+): (\w+)\((\d+)\)(.*)\| mat=\(([\d,]*)\) sets=\(([\d,]*)\)$")
+    for q in range(14):
+        for prog in sme.plan_describe(q, plan_type).split("program Q")[1:]:
+            live, mat = set(), set()
+            for line in prog.strip().splitlines()[1:]:
+                m = step_re.match(line.strip())
+                assert m, line
+                kind, u, rest = m.group(2), int(m.group(3)), m.group(4)
+                r = re.search(r"reuse=(\d+)", rest)
+                if r:
+                    assert int(r.group(1)) in live, (q, plan_type, line)
+                c = re.search(r"conn=\(([\d,]+)\)", rest)
+                if c:
+                    assert {int(x) for x in c.group(1).split(",")} <= mat, (q, plan_type, line)
+                mat = {int(x) for x in m.group(5).split(",") if x}
+                live = {int(x) for x in m.group(6).split(",") if x}
