@@ -33,6 +33,8 @@ REF = os.path.join(ROOT, "oracle", "_ref")
 GRAPHS = {
     "k6": lambda: sme.Graph.clique(6),
     "k12": lambda: sme.Graph.clique(12),
+    # the reference's own K20 cross-check graph (TestPatternMatchCPU.cpp:97-147)
+    "k20": lambda: sme.Graph.clique(20),
     "rmat_s8_ef8": lambda: sme.Graph.rmat(8, 8, seed=11),
     "rmat_s10_ef8": lambda: sme.Graph.rmat(10, 8, seed=12),
     "rmat_s12_ef8": lambda: sme.Graph.rmat(12, 8, seed=13),

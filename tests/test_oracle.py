@@ -18,6 +18,19 @@ def test_k6_closed_forms(golden):
     assert (c["0"], c["1"], c["2"], c["3"], c["4"], c["7"]) == (20, 45, 90, 15, 360, 6)
 
 
+def test_k20_reference_counts_and_closed_forms(golden):
+    # K20 is the reference's own cross-check graph (its Q5 count must agree
+    # between the CPU algorithms, TestPatternMatchCPU.cpp:97-147); the clique
+    # counts are binomials, the 4-cycle 3*C(n,4), the diamond 6*C(n,4), the
+    # house 5!/2 * C(n,5)
+    from math import comb
+    c = golden["k20"]["counts"]
+    assert c["0"] == comb(20, 3) and c["3"] == comb(20, 4) and c["7"] == comb(20, 5) and c["11"] == comb(20, 6)
+    assert c["1"] == 3 * comb(20, 4) and c["2"] == 6 * comb(20, 4) and c["4"] == 60 * comb(20, 5)
+    rp, cl = O.read_bin(golden_graph_path("k20"))
+    assert O.count(rp, cl, 5) == c["5"] == 13953600
+
+
 def test_oracle_matches_reference_counts(golden):
     checked = 0
     for name, d in golden.items():
