@@ -127,7 +127,12 @@ sme_status sme_graph_load_bin(const char* path, sme_graph** out);
 /* SNAP edge list text (GraphIO.h:195-270); directed=0 stores both directions;
  * adjacency lists are sorted.  No preprocessing. */
 sme_status sme_graph_load_snap(const char* path, int directed, sme_graph** out);
-/* Dispatch on the file suffix like GraphIO::ReadDataFile (GraphIO.h:48-64). */
+/* SNAP edge list whose vertex names are any digit strings
+ * (GraphIO::ReadSNAPLargeVIDFile, GraphIO.h:142-230): names get dense ids in
+ * order of first appearance; lists sorted; no preprocessing. */
+sme_status sme_graph_load_snap_lvid(const char* path, int directed, sme_graph** out);
+/* Dispatch on the file suffix like GraphIO::ReadDataFile (GraphIO.h:48-64):
+ * .txt SNAP, .bin BIN, .lvid SNAP with large vertex ids. */
 sme_status sme_graph_load(const char* path, int directed, sme_graph** out);
 /* From caller CSR.  copy=1 copies; copy=0 borrows (caller keeps the arrays
  * alive and unchanged until sme_graph_free). */
@@ -140,6 +145,14 @@ sme_status sme_graph_csr(const sme_graph* g, const uint64_t** row_ptrs,
                          const uint32_t** cols);
 /* Writes exactly the bytes of GraphIO::WriteCSRBinFile to `path`. */
 sme_status sme_graph_write_bin(const sme_graph* g, const char* path);
+/* Writes exactly the text of GraphIO::WriteCSRSNAPFile (GraphIO.h:389-413):
+ * "u v" per edge with u < v.  The reference appends ".snap.txt" to its
+ * input name; here `path` is used as given. */
+sme_status sme_graph_write_snap(const sme_graph* g, const char* path);
+/* Writes exactly the text of GraphIO::WriteCSRAdjFile (GraphIO.h:414-436),
+ * the partitioner's input: "u<TAB>v v ... " per vertex, and `path`.info with
+ * "n m".  The reference appends ".adj.txt"; here `path` is used as given. */
+sme_status sme_graph_write_adj(const sme_graph* g, const char* path);
 /* PreprocessGraph::Preprocess: drop self loops and parallel edges, then
  * dangling vertices with a dense order-preserving relabel. */
 sme_status sme_graph_preprocess(sme_graph* g);

@@ -102,6 +102,9 @@ SIGNATURES = {
     "sme_graph_validate": (C.c_int, [_P]),
     "sme_graph_degree_order": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_void_p), C.c_void_p]),
     "sme_read_partition_file": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint32, C.c_void_p]),
+    "sme_graph_load_snap_lvid": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "sme_graph_write_snap": (C.c_int, [_P, C.c_char_p]),
+    "sme_graph_write_adj": (C.c_int, [_P, C.c_char_p]),
     "sme_graph_partition": (C.c_int, [_P, C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
     "sme_count_partitioned": (C.c_int, [_P, C.POINTER(Opts), C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64),
                                         C.c_void_p]),
@@ -262,6 +265,13 @@ class Graph:
 
     def write_bin(self, path: str) -> None:
         _check(lib().sme_graph_write_bin(self._h, path.encode()))
+
+    def write_snap(self, path: str) -> None:
+        _check(lib().sme_graph_write_snap(self._h, path.encode()))
+
+    def write_adj(self, path: str) -> None:
+        """`path` and `path`.info (n m), the partitioner's input format."""
+        _check(lib().sme_graph_write_adj(self._h, path.encode()))
 
     def preprocess(self) -> None:
         _check(lib().sme_graph_preprocess(self._h))

@@ -184,14 +184,34 @@ sme_status sme_graph_load_snap(const char* path, int directed, sme_graph** out) 
   });
 }
 
+sme_status sme_graph_load_snap_lvid(const char* path, int directed, sme_graph** out) {
+  if (!path || !out) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    std::unique_ptr<sme_graph> g(new sme_graph());
+    ReadSnapLvidFile(path, directed != 0, g->g);
+    *out = g.release();
+  });
+}
+
 sme_status sme_graph_load(const char* path, int directed, sme_graph** out) {
   if (!path || !out) return SME_ERR_INVALID_ARG;
   std::string p(path);
   std::string suf = p.substr(p.rfind('.') + 1);
   if (suf == "bin") return sme_graph_load_bin(path, out);
   if (suf == "txt") return sme_graph_load_snap(path, directed, out);
-  SetLastError("unknown graph file suffix ." + suf + " (expected .bin or .txt)");
+  if (suf == "lvid") return sme_graph_load_snap_lvid(path, directed, out);
+  SetLastError("unknown graph file suffix ." + suf + " (expected .bin, .txt or .lvid)");
   return SME_ERR_BAD_FILE;
+}
+
+sme_status sme_graph_write_snap(const sme_graph* g, const char* path) {
+  if (!g || !path) return SME_ERR_INVALID_ARG;
+  return Guard([&] { WriteSnapFile(path, g->g); });
+}
+
+sme_status sme_graph_write_adj(const sme_graph* g, const char* path) {
+  if (!g || !path) return SME_ERR_INVALID_ARG;
+  return Guard([&] { WriteAdjFile(path, g->g); });
 }
 
 sme_status sme_graph_from_csr(const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n, uint64_t m, int copy,

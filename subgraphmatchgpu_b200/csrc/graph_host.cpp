@@ -8,10 +8,12 @@
 //   validate         src/graph/GraphIO.h:459-485
 // The reader does one bulk read per array instead of one fread per element.
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <fstream>
 #include <sstream>
+#include <unordered_map>
 
 #include "sme_internal.h"
 
@@ -148,6 +150,80 @@ void ReadSnapFile(const std::string& path, bool directed, HostGraph& g) {
   }
   SortLists(n, r.data(), c.data());
   g.Adopt(std::move(r), std::move(c));
+}
+
+// SNAP edge list with arbitrary vertex names (GraphIO::ReadSNAPLargeVIDFile,
+// src/graph/GraphIO.h:142-230): every run of digits on a line that starts
+// with a digit is a vertex name; names get dense ids in order of first
+// appearance (the exact string: "007" and "7" are two vertices); the names
+// pair up into edges in order.  Lists are sorted; nothing is deduplicated.
+void ReadSnapLvidFile(const std::string& path, bool directed, HostGraph& g) {
+  std::ifstream in(path);
+  if (!in) Fail(SME_ERR_BAD_FILE, "cannot open " + path);
+  std::unordered_map<std::string, uintV> ids;
+  std::vector<uintV> ends;
+  std::string line;
+  while (std::getline(in, line)) {
+    if (line.empty() || !std::isdigit((unsigned char)line[0])) continue;
+    size_t i = 0;
+    while (i < line.size()) {
+      while (i < line.size() && !std::isdigit((unsigned char)line[i])) ++i;
+      size_t j = i;
+      while (j < line.size() && std::isdigit((unsigned char)line[j])) ++j;
+      if (j > i) {
+        auto it = ids.emplace(line.substr(i, j - i), (uintV)ids.size()).first;
+        ends.push_back(it->second);
+      }
+      i = j;
+    }
+  }
+  if (ends.size() % 2) Fail(SME_ERR_BAD_FILE, "odd number of vertex names in " + path);
+  const uint64_t n = ids.size();
+  std::vector<uintE> r(n + 1, 0);
+  for (size_t k = 0; k < ends.size(); k += 2) {
+    r[ends[k] + 1]++;
+    if (!directed) r[ends[k + 1] + 1]++;
+  }
+  for (uint64_t u = 0; u < n; ++u) r[u + 1] += r[u];
+  std::vector<uintV> c(r[n]);
+  std::vector<uintE> pos(r.begin(), r.end() - 1);
+  for (size_t k = 0; k < ends.size(); k += 2) {
+    c[pos[ends[k]]++] = ends[k + 1];
+    if (!directed) c[pos[ends[k + 1]]++] = ends[k];
+  }
+  SortLists(n, r.data(), c.data());
+  g.Adopt(std::move(r), std::move(c));
+}
+
+// GraphIO::WriteCSRSNAPFile (src/graph/GraphIO.h:389-413): "u v" per stored
+// pair with u < v, in CSR order.
+void WriteSnapFile(const std::string& path, const HostGraph& g) {
+  std::ofstream out(path);
+  if (!out) Fail(SME_ERR_BAD_FILE, "cannot create " + path);
+  for (uint64_t u = 0; u < g.n; ++u)
+    for (uintE j = g.row_ptrs[u]; j < g.row_ptrs[u + 1]; ++j)
+      if (u < g.cols[j]) out << u << " " << g.cols[j] << "\n";
+  if (!out) Fail(SME_ERR_BAD_FILE, "write failed: " + path);
+}
+
+// GraphIO::WriteCSRAdjFile (src/graph/GraphIO.h:414-436), the partitioner's
+// input: per vertex "u<TAB>" then "v " per neighbour, then a newline; and
+// `path`.info holding "n m".
+void WriteAdjFile(const std::string& path, const HostGraph& g) {
+  {
+    std::ofstream out(path);
+    if (!out) Fail(SME_ERR_BAD_FILE, "cannot create " + path);
+    for (uint64_t u = 0; u < g.n; ++u) {
+      out << u << "\t";
+      for (uintE j = g.row_ptrs[u]; j < g.row_ptrs[u + 1]; ++j) out << g.cols[j] << " ";
+      out << "\n";
+    }
+    if (!out) Fail(SME_ERR_BAD_FILE, "write failed: " + path);
+  }
+  std::ofstream info(path + ".info");
+  if (!info) Fail(SME_ERR_BAD_FILE, "cannot create " + path + ".info");
+  info << g.n << " " << g.m;
+  if (!info) Fail(SME_ERR_BAD_FILE, "write failed: " + path + ".info");
 }
 
 // ------------------------------------------------------------ preprocess --

@@ -53,6 +53,9 @@ struct HostGraph {
 void ReadBinFile(const std::string& path, HostGraph& g);
 void ReadSnapFile(const std::string& path, bool directed, HostGraph& g);
 void WriteBinFile(const std::string& path, const HostGraph& g);
+void ReadSnapLvidFile(const std::string& path, bool directed, HostGraph& g);
+void WriteSnapFile(const std::string& path, const HostGraph& g);
+void WriteAdjFile(const std::string& path, const HostGraph& g);
 void Preprocess(HostGraph& g);
 void Validate(const HostGraph& g);
 // Builds a sorted undirected CSR from an edge list (both directions stored),

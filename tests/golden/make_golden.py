@@ -10,8 +10,13 @@ has the reference sources; the outputs are committed).
 * preprocess.json  SHA-256 of the BIN file the reference's `preprocess_graph`
                  writes for a messy SNAP edge list, and of libsme's result for
                  the same text (they must be identical)
+* formats.json   SHA-256 of what the reference's `preprocess_graph` writes
+                 as SNAP text (-o 0) and as ADJ text + info (-o 3) for that
+                 edge list, and as BIN for an edge list with large, zero-padded
+                 vertex names read through its .lvid reader (messy.lvid)
 
-Usage:  python tests/golden/make_golden.py   (after `make -C oracle ref`)
+Usage:  python tests/golden/make_golden.py [formats]   (after `make -C oracle ref`;
+        `formats` regenerates formats.json and messy.lvid only)
 """
 import hashlib
 import json
@@ -115,5 +120,56 @@ def main():
     print("preprocess", res)
 
 
+def formats():
+    """The other graph formats of GraphIO, pinned against preprocess_graph."""
+    res = {}
+    messy = os.path.join(HERE, "messy_edges.txt")
+    rnd = random.Random(9)
+    names = [str(rnd.randrange(10 ** 9, 10 ** 14)) for _ in range(150)] + ["7", "007", "0", "00"]
+    lines = ["# vertex names beyond 32 bits, zero-padded duplicates of small ids"]
+    for _ in range(1200):
+        u, v = rnd.choice(names), rnd.choice(names)
+        sep = rnd.choice(["\t", " ", ", ", " ; "])
+        lines.append(f"{u}{sep}{v}")
+    lvid = os.path.join(HERE, "messy.lvid")
+    with open(lvid, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    with tempfile.TemporaryDirectory() as td:
+        txt = os.path.join(td, "messy.txt")
+        with open(messy) as src, open(txt, "w") as dst:
+            dst.write(src.read())
+        for fmt, suffix in ((0, ".snap.txt"), (3, ".adj.txt")):
+            subprocess.run([os.path.join(REF, "preprocess_graph"), "-f", txt, "-d", "0", "-o", str(fmt)],
+                           capture_output=True, check=True)
+            res[f"reference{suffix}"] = sha(txt + suffix)
+        with open(txt + ".adj.txt.info") as f:
+            res["reference.adj.txt.info"] = f.read()
+        g = sme.Graph.load(txt, 0)
+        g.preprocess()
+        g.write_snap(os.path.join(td, "mine.snap"))
+        g.write_adj(os.path.join(td, "mine.adj"))
+        res["libsme.snap.txt"] = sha(os.path.join(td, "mine.snap"))
+        res["libsme.adj.txt"] = sha(os.path.join(td, "mine.adj"))
+        with open(os.path.join(td, "mine.adj.info")) as f:
+            res["libsme.adj.txt.info"] = f.read()
+        tl = os.path.join(td, "messy.lvid")
+        with open(lvid) as src, open(tl, "w") as dst:
+            dst.write(src.read())
+        subprocess.run([os.path.join(REF, "preprocess_graph"), "-f", tl, "-d", "0", "-o", "1"],
+                       capture_output=True, check=True)
+        res["reference.lvid.bin"] = sha(tl + ".bin")
+        g = sme.Graph.load(tl, 0)
+        g.preprocess()
+        g.write_bin(os.path.join(td, "mine_lvid.bin"))
+        res["libsme.lvid.bin"] = sha(os.path.join(td, "mine_lvid.bin"))
+    with open(os.path.join(HERE, "formats.json"), "w") as f:
+        json.dump(res, f, indent=1, sort_keys=True)
+    print("formats", res)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["formats"]:
+        formats()
+    else:
+        main()
+        formats()

@@ -293,3 +293,34 @@ def test_reused_sets_are_live_where_they_are_read(plan_type):
                     assert {int(x) for x in c.group(1).split(",")} <= mat, (q, plan_type, line)
                 mat = {int(x) for x in m.group(5).split(",") if x}
                 live = {int(x) for x in m.group(6).split(",") if x}
+
+
+def test_snap_adj_and_lvid_formats_match_reference_preprocess_graph(tmp_path):
+    # pinned by tests/golden/make_golden.py against the reference's
+    # preprocess_graph (-o 0 SNAP text, -o 3 ADJ text + info, .lvid input)
+    rec = json.load(open(os.path.join(ROOT, "tests", "golden", "formats.json")))
+    g = sme.Graph.load(os.path.join(ROOT, "tests", "golden", "messy_edges.txt"), 0)
+    g.preprocess()
+    g.write_snap(str(tmp_path / "g.snap"))
+    g.write_adj(str(tmp_path / "g.adj"))
+    assert sha(str(tmp_path / "g.snap")) == rec["reference.snap.txt"]
+    assert sha(str(tmp_path / "g.adj")) == rec["reference.adj.txt"]
+    assert (tmp_path / "g.adj.info").read_text() == rec["reference.adj.txt.info"]
+    lv = sme.Graph.load(os.path.join(ROOT, "tests", "golden", "messy.lvid"), 0)
+    lv.preprocess()
+    lv.write_bin(str(tmp_path / "lvid.bin"))
+    assert sha(str(tmp_path / "lvid.bin")) == rec["reference.lvid.bin"]
+
+
+def test_lvid_names_are_exact_strings(tmp_path):
+    f = tmp_path / "x.lvid"
+    f.write_text("# names\n7 007\n007 123456789012345\n123456789012345,7\n")
+    g = sme.Graph.load(str(f), 0)
+    # 7 -> 0, 007 -> 1, 123456789012345 -> 2: a triangle
+    assert g.info()[:2] == (3, 6)
+    rp, cl = g.csr()
+    assert rp.tolist() == [0, 2, 4, 6] and cl.tolist() == [1, 2, 0, 2, 0, 1]
+    f.write_text("1 2 3\n")
+    with pytest.raises(sme.SmeError) as e:
+        sme.Graph.load(str(f), 0)
+    assert e.value.status == 2
