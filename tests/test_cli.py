@@ -71,3 +71,32 @@ def test_hybrid_mode_result_lines(golden, tmp_path):
     inter = int(re.search(r"^inter_partition_count=(\d+)$", r.stdout, re.M).group(1))
     total = int(re.search(r"^total_match_count=(\d+), elapsed_time=", r.stdout, re.M).group(1))
     assert len(intra) == 3 and total == golden[name]["counts"]["3"] and sum(intra) + inter == total
+
+
+def test_preprocess_graph_tool_writes_what_the_reference_tool_writes(tmp_path):
+    # same flags and output names as the reference's preprocess_graph; the
+    # hashes were taken from the reference tool (tests/golden/make_golden.py)
+    import hashlib
+    import json
+    import shutil
+    tool = os.path.join(ROOT, "subgraphmatchgpu_b200", "bin", "preprocess_graph")
+    golden = os.path.join(ROOT, "tests", "golden")
+    pre = json.load(open(os.path.join(golden, "preprocess.json")))
+    fmt = json.load(open(os.path.join(golden, "formats.json")))
+    txt = tmp_path / "messy.txt"
+    shutil.copy(os.path.join(golden, "messy_edges.txt"), txt)
+    lvid = tmp_path / "messy.lvid"
+    shutil.copy(os.path.join(golden, "messy.lvid"), lvid)
+
+    def sha(p):
+        return hashlib.sha256(open(p, "rb").read()).hexdigest()
+
+    for args, out, want in (((txt, 1), str(txt) + ".bin", pre["reference_sha256"]),
+                            ((txt, 0), str(txt) + ".snap.txt", fmt["reference.snap.txt"]),
+                            ((txt, 3), str(txt) + ".adj.txt", fmt["reference.adj.txt"]),
+                            ((lvid, 1), str(lvid) + ".bin", fmt["reference.lvid.bin"])):
+        r = subprocess.run([tool, "-f", str(args[0]), "-d", "0", "-o", str(args[1])], capture_output=True,
+                           text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        assert sha(out) == want, out
+    assert open(str(txt) + ".adj.txt.info").read() == fmt["reference.adj.txt.info"]
