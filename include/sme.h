@@ -90,7 +90,12 @@ typedef struct sme_opts {
                               (default) starts a set from an earlier
                               candidate set that covers some of its lists
                               when the conditions allow (same sets)        */
-  int32_t reserved[4];
+  const uint32_t* roots;   /* explicit root task: when num_roots > 0 the
+                              first level is exactly roots[0..num_roots)
+                              (host memory, ids below n; a root listed
+                              twice counts twice) and root_begin / root_end
+                              / root_stride are ignored                    */
+  uint64_t num_roots;
 } sme_opts;
 
 /* Counters of the last sme_count/sme_enumerate call on this thread. */
@@ -101,7 +106,12 @@ typedef struct sme_stats {
   double kernel_ms;           /* sum of CUDA-event time of the hot kernels   */
   uint64_t kernel_launches;   /* kernels of this library launched            */
   uint64_t batches;           /* level batches processed                    */
-  uint64_t algorithmic_bytes; /* merge-bound bytes of all intersection steps */
+  uint64_t algorithmic_bytes; /* bytes the intersection steps must touch: per
+                                 path 12 per backward list (row pointers +
+                                 gathered vertex), 4 x clipped pivot length x
+                                 lists intersected (each pivot element read
+                                 once and tested once per other list), 4 per
+                                 candidate written                           */
   uint64_t h2d_bytes;         /* host->device bytes moved by this call       */
   uint64_t d2h_bytes;
   uint64_t peak_device_bytes; /* high-water mark of the frontier arena       */
@@ -267,19 +277,26 @@ sme_status sme_batch_free(sme_batch_plan* p);
 
 /* Allocation-free count of query `query_type` on one graph whose CSR the
  * caller already holds in device memory (d_row_ptrs: n+1 uint64 offsets,
- * d_cols: uint32 neighbour ids, sorted lists, both directions stored).  It has
- * no counterpart in the reference.  It exists for callers that must not call
- * cudaMalloc: code running under a framework whose caching allocator already
- * owns the device memory, or latency-critical paths that cannot afford an
- * allocation and the synchronisation it implies.  Besides the caller's
- * buffers it uses only a 16 MiB array the library reserves in device memory
- * for the life of the process on every GPU that loads it; nothing is
- * allocated or freed.  Limit: the graph's maximum degree must be at most
- * 32768 and n below 2^31, else SME_ERR_CAPACITY / SME_ERR_INVALID_ARG.
+ * d_cols: uint32 neighbour ids; every list strictly increasing, so sorted with
+ * no duplicate neighbours, no self loops, ids below n, both directions
+ * stored).  It has no counterpart in the reference.  It exists for callers
+ * that must not call cudaMalloc: code running under a framework whose caching
+ * allocator already owns the device memory, or latency-critical paths that
+ * cannot afford an allocation and the synchronisation it implies.  Besides
+ * the caller's buffers it uses only a 16 MiB array the library reserves in
+ * device memory for the life of the process on every GPU that loads it;
+ * nothing is allocated or freed.  Limit: the graph's maximum degree must be
+ * at most 32768 and n below 2^31, else SME_ERR_CAPACITY / SME_ERR_INVALID_ARG;
+ * a list that breaks the contract above returns SME_ERR_INVALID_ARG (checked
+ * on the device in the same pass that finds the maximum degree).  The number
+ * of thread groups the array holds falls as the maximum degree rises (about
+ * 7 blocks of 16 groups at the limit), so hub-heavy graphs count slowly here.
  * The first call on a device looks up the array's device address, so make
- * that first call before any stream capture.  Calls run on the legacy default
- * stream and return when the count is known; all calls share the one array,
- * so calls that overlap on the same GPU (from several host threads) race. */
+ * that first call before any stream capture.  Every call clears the array's
+ * header with cudaMemsetAsync on the legacy default stream, launches its
+ * kernels there and reads results back with two blocking cudaMemcpy; it
+ * returns when the count is known.  All calls share the one array, so calls
+ * that overlap on the same GPU (from several host threads) race. */
 sme_status sme_count_noalloc(const uint64_t* d_row_ptrs, const uint32_t* d_cols,
                              uint64_t n, int32_t query_type, uint64_t* count);
 

@@ -401,3 +401,47 @@ uint64_t oracle_wcoj_sample(const uint64_t* rp, const uint32_t* cols, uint64_t n
   if (done) *done = completed;
   return total;
 }
+
+/*
+ * Writes an edge list as SNAP text ("u v\n" per edge, decimal), the input
+ * format of the reference's preprocess_graph tool (GraphIO.h:232-270): a
+ * fast writer for the benchmark's generated edge lists.  Returns 0 on
+ * success.
+ */
+#include <stdio.h>
+int oracle_write_edge_text(const uint32_t* u, const uint32_t* v, uint64_t ne, const char* path) {
+  FILE* f = fopen(path, "wb");
+  if (!f) return 1;
+  enum { CAP = 1 << 22 };
+  char* buf = (char*)malloc(CAP + 32);
+  if (!buf) {
+    fclose(f);
+    return 1;
+  }
+  size_t len = 0;
+  for (uint64_t i = 0; i < ne; ++i) {
+    uint32_t x[2] = {u[i], v[i]};
+    for (int k = 0; k < 2; ++k) {
+      char tmp[12];
+      int t = 0;
+      uint32_t y = x[k];
+      do {
+        tmp[t++] = (char)('0' + y % 10);
+        y /= 10;
+      } while (y);
+      while (t) buf[len++] = tmp[--t];
+      buf[len++] = k == 0 ? ' ' : '\n';
+    }
+    if (len >= CAP) {
+      if (fwrite(buf, 1, len, f) != len) {
+        free(buf);
+        fclose(f);
+        return 1;
+      }
+      len = 0;
+    }
+  }
+  int bad = len && fwrite(buf, 1, len, f) != len;
+  free(buf);
+  return fclose(f) != 0 || bad;
+}

@@ -51,7 +51,7 @@ class Opts(C.Structure):
         ("reuse_autogen", C.c_int32), ("device", C.c_int32), ("mem_limit_bytes", C.c_uint64),
         ("root_begin", C.c_uint64), ("root_end", C.c_uint64), ("warp_granularity", C.c_int32),
         ("list_only", C.c_int32), ("root_stride", C.c_uint32), ("no_set_reuse", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("roots", C.c_void_p), ("num_roots", C.c_uint64),
     ]
 
 
@@ -164,9 +164,17 @@ def _check(st: int) -> None:
 
 
 def opts(query: int = 0, algo: int = GPU_LIGHT, mode: int = IN_MEMORY_GPU, **kw) -> Opts:
+    """sme_opts with the library defaults; `roots` (a sequence of vertex
+    ids) makes the run an explicit root task, kept alive with the struct."""
     o = Opts()
     _check(lib().sme_opts_default(C.byref(o)))
     o.query_type, o.algo, o.execute_mode = query, algo, mode
+    roots = kw.pop("roots", None)
+    if roots is not None:
+        r = np.ascontiguousarray(roots, dtype=np.uint32)
+        o._roots = r
+        o.roots = r.ctypes.data if len(r) else None
+        o.num_roots = len(r)
     for k, v in kw.items():
         setattr(o, k, v)
     return o

@@ -306,8 +306,13 @@ BProg CompileBatchProgram(int q) {
   return p;
 }
 
+// Uploads the 14 level programs to the current device once per device; host
+// threads preparing batches or allocation-free counts on the same device at
+// the same time serialise here.
 void UploadPrograms(int device) {
+  static std::mutex mu;
   static bool done[64] = {false};
+  std::lock_guard<std::mutex> l(mu);
   if (device >= 0 && device < 64 && done[device]) return;
   BProg all[SME_NUM_QUERIES];
   for (int q = 0; q < SME_NUM_QUERIES; ++q) all[q] = CompileBatchProgram(q);
@@ -330,24 +335,49 @@ int MaxBuffers(const std::vector<int32_t>& queries) {
 // Library-owned device memory, reserved when the library is loaded and kept
 // by every GPU that loads it until the process exits: 16 MiB.  Words [0,64)
 // hold one call's control values (word 0: next work item, words 2-3: the
-// uint64 count, word 4: the graph's maximum degree); the rest holds the
-// thread groups' level buffers.  Every call reuses (and first clears) it.
+// uint64 count, word 4: the graph's maximum degree, word 5: set when a list
+// is unsorted, holds a duplicate, a self loop or an id >= n); the rest holds
+// the thread groups' level buffers.  Every call reuses (and first clears) it.
 constexpr size_t kNoAllocWords = size_t(4) << 20;
 constexpr size_t kNoAllocHeader = 64;
 constexpr uint32_t kNoAllocMaxDegree = 32768;
 constexpr int kNoAllocGroup = 8;
 constexpr int kNoAllocBlock = 128;
+// At the maximum degree, the level buffers of the deepest program (at most
+// BMAXV - 2 buffered levels) must still fit one block of thread groups.
+static_assert((kNoAllocWords - kNoAllocHeader) / ((size_t)(BMAXV - 2) * kNoAllocMaxDegree) >=
+                  (size_t)(kNoAllocBlock / kNoAllocGroup),
+              "allocation-free scratch must hold at least one block of level buffers");
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
 
-__global__ void k_noalloc_maxdeg(const uint64_t* __restrict__ rp, uint32_t n, unsigned int* out) {
+// One pass over the caller's CSR: the maximum degree (word 4 of `hdr`) and
+// the input contract of the sorted-list searches (word 5: 1 when a list is
+// not strictly increasing, holds its own vertex or an id >= n).
+__global__ void k_noalloc_inspect(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ cols, uint32_t n,
+                                  unsigned int* hdr) {
   unsigned int m = 0;
+  bool bad = false;
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    uint64_t d = rp[v + 1] - rp[v];
+    const uint64_t b = rp[v], e = rp[v + 1];
+    const uint64_t d = e - b;  // wraps to a huge degree when e < b
     m = max(m, (unsigned int)min(d, (uint64_t)0xffffffffu));
+    if (e < b || d > kNoAllocMaxDegree) continue;  // refused on the degree alone
+    uint32_t prev = 0;
+    for (uint64_t i = b; i < e; ++i) {
+      const uint32_t x = __ldg(cols + i);
+      bad = bad || x >= n || x == v || (i > b && x <= prev);
+      prev = x;
+    }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(FULL, m, o));
-  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+  for (int o = 16; o > 0; o >>= 1) {
+    m = max(m, __shfl_down_sync(FULL, m, o));
+    bad = bad || __shfl_down_sync(FULL, (int)bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (m) atomicMax(hdr + 4, m);
+    if (bad) atomicOr(hdr + 5, 1u);
+  }
 }
 
 // The batched form's depth-first enumeration for one graph with 64-bit row
@@ -434,15 +464,21 @@ uint64_t CountNoAlloc(const uint64_t* d_rp, const uint32_t* d_cols, uint64_t n, 
   const uint32_t nv = (uint32_t)n;
   int sms = 148;
   BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  k_noalloc_maxdeg<<<sms * 4, 256, 0, 0>>>(d_rp, nv, base + 4);
-  uint32_t maxdeg = 0;
-  BCK(cudaMemcpy(&maxdeg, base + 4, sizeof(maxdeg), cudaMemcpyDeviceToHost));
+  k_noalloc_inspect<<<sms * 4, 256, 0, 0>>>(d_rp, d_cols, nv, base);
+  uint32_t hdr[8] = {0};
+  BCK(cudaMemcpy(hdr, base, sizeof(hdr), cudaMemcpyDeviceToHost));
+  const uint32_t maxdeg = hdr[4];
   if (maxdeg > kNoAllocMaxDegree)
     Fail(SME_ERR_CAPACITY, "sme_count_noalloc: maximum degree " + std::to_string(maxdeg) +
                                " exceeds the allocation-free limit " + std::to_string(kNoAllocMaxDegree));
+  if (hdr[5])
+    Fail(SME_ERR_INVALID_ARG, "sme_count_noalloc: every adjacency list must be strictly increasing, hold ids "
+                              "below n and not its own vertex (sorted, no duplicates, no self loops)");
   const uint32_t nbuf = (uint32_t)MaxBuffers({q});
   const uint32_t cap = std::max<uint32_t>(maxdeg, 1);
   const size_t groups_fit = (kNoAllocWords - kNoAllocHeader) / ((size_t)nbuf * cap);
+  if (nbuf > BMAXV - 2 || groups_fit < (size_t)(kNoAllocBlock / kNoAllocGroup))
+    Fail(SME_ERR_CAPACITY, "sme_count_noalloc: level buffers exceed the allocation-free scratch");
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_noalloc_dfs<kNoAllocGroup>, kNoAllocBlock, 0);
   const size_t gpb = kNoAllocBlock / kNoAllocGroup;

@@ -62,6 +62,25 @@ static void CheckOpts(const sme_opts& o) {
     Fail(SME_ERR_INVALID_ARG, "EXTERNAL_GPU runs the LIGHT plan only (algo 6)");
 }
 
+RootTask TaskOf(const sme_opts& o, uint64_t n) {
+  RootTask t;
+  if (o.num_roots > 0) {
+    if (!o.roots) Fail(SME_ERR_INVALID_ARG, "num_roots > 0 with a null roots array");
+    for (uint64_t i = 0; i < o.num_roots; ++i)
+      if (o.roots[i] >= n)
+        Fail(SME_ERR_INVALID_ARG, "roots[" + std::to_string(i) + "] = " + std::to_string(o.roots[i]) +
+                                      " is not a vertex (n = " + std::to_string(n) + ")");
+    t.list = o.roots;
+    t.list_len = o.num_roots;
+    return t;
+  }
+  t.begin = o.root_begin;
+  t.end = o.root_end ? std::min<uint64_t>(o.root_end, n) : n;
+  if (t.begin > t.end) t.begin = t.end;
+  t.stride = o.root_stride ? o.root_stride : 1;
+  return t;
+}
+
 struct RunOut {
   uint64_t count = 0;
   uint64_t emitted = 0;
@@ -84,13 +103,12 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
     slot.bytes = o.mem_limit_bytes;
   }
   DeviceContext& ctx = *slot.ctx;
-  uint64_t rb = o.root_begin, re = o.root_end ? o.root_end : g->g.n;
-  if (re > g->g.n) re = g->g.n;
+  const RootTask task = TaskOf(o, g->g.n);
   RunResult r;
   uint64_t h2d = 0, d2h = 8;
   if (o.execute_mode == SME_EXTERNAL_GPU) {
     if (enumerate) Fail(SME_ERR_INVALID_ARG, "enumeration runs in IN_MEMORY_GPU mode");
-    r = RunProgramExternal(prog, g->g, ctx, rb, re, o.ext_variant, 0, o.root_stride);
+    r = RunProgramExternal(prog, g->g, ctx, task, o.ext_variant, 0);
     h2d = r.stats.h2d_bytes;
   } else {
     DeviceGraph* dg = g->g.dev;
@@ -116,7 +134,7 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
           Fail(SME_ERR_OOM, "cannot allocate enumeration buffer");
         }
       }
-      r = RunProgram(prog, *dg, ctx, rb, re, d_out, cap, Tuning(o), o.root_stride);
+      r = RunProgram(prog, *dg, ctx, task, d_out, cap, Tuning(o));
       if (enumerate && cap && host_out) {
         uint64_t ncopy = std::min<uint64_t>(r.emitted, cap);
         if (ncopy) {
@@ -136,6 +154,7 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
     if (temp) FreeDeviceGraph(dg);
     ctx.arena.Release(graph_mark);
   }
+  if (o.execute_mode != SME_EXTERNAL_GPU) h2d += r.stats.h2d_bytes;  // the root list
   r.stats.h2d_bytes = h2d;
   r.stats.d2h_bytes = d2h;
   r.stats.elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -250,13 +250,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
         if (i == nl) GetSet(F, s.reuse, p, L[i], N[i]);
       ++nl;
     }
-    if (lane == 0) {
-      uint64_t b = 12ULL * s.nconn;
-#pragma unroll
-      for (int i = 0; i < NLM; ++i)
-        if (i < nl) b += 4ULL * N[i];
-      bytes += b;
-    }
+    if (lane == 0) bytes += 12ULL * s.nconn;  // row pointers + gathered instance vertices
     // pivot to slot 0
 #pragma unroll
     for (int i = 1; i < NLM; ++i) {
@@ -288,7 +282,6 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
           if (lane == 0) {
             out_ptr[p] = (uint64_t)(L[0] + r0);
             out_cnt[p] = r1 - r0;
-            bytes += 4ULL * (r1 - r0);
           }
           continue;
         }
@@ -299,6 +292,9 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     uint32_t WN = 0;
     if (MODE == 1 && s.with_u >= 0) GetSet(F, s.with_u, p, W, WN);
 
+    // every element of the clipped pivot is read once and tested against
+    // each other list (one bitmap word or one list element answers a test)
+    if (lane == 0) bytes += 4ULL * (r1 - r0) * (uint64_t)nl;
     uint32_t cur[NLM];
 #pragma unroll
     for (int i = 0; i < NLM; ++i) cur[i] = 0;
@@ -421,10 +417,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute_flat(
           if (i == nl) GetSet(F, s.reuse, p, L[i], N[i]);
         ++nl;
       }
-      uint64_t b = 12ULL * s.nconn;
-#pragma unroll
-      for (int i = 0; i < NLM; ++i)
-        if (i < nl) b += 4ULL * N[i];
+      uint64_t b = 12ULL * s.nconn;  // row pointers + gathered instance vertices
 #pragma unroll
       for (int i = 1; i < NLM; ++i) {
         if (i < nl && N[i] < N[0]) {
@@ -449,11 +442,11 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute_flat(
           if (Exclusions(L[0], r0, r1, bd, ex) == 0) {
             out_ptr[p] = (uint64_t)(L[0] + r0);
             out_cnt[p] = r1 - r0;
-            b += 4ULL * (r1 - r0);
             view = true;
           }
         }
       }
+      if (!view) b += 4ULL * (r1 - r0) * (uint64_t)nl;  // pivot elements x lists tested
       bytes += b;
       fp.W = nullptr;
       fp.WN = 0;
@@ -1041,8 +1034,8 @@ class Executor {
   void SetExternal(const uint32_t* host_cols) { ext_cols_ = host_cols; }
   uint64_t ext_h2d_bytes() const { return ext_bytes_; }
 
-  RunResult Run(uint64_t rb, uint64_t re, uint32_t stride = 1) {
-    if (stride == 0) stride = 1;
+  RunResult Run(const RootTask& task) {
+    const uint32_t stride = task.stride ? task.stride : 1;
     auto t0 = std::chrono::steady_clock::now();
     size_t mark = A_.Mark();
     A_.peak = mark;  // high-water mark of this run
@@ -1053,19 +1046,23 @@ class Executor {
     CK(cudaEventRecord(ev0, st_));
     CK(cudaMemsetAsync(ctrl_, 0, 8 * sizeof(unsigned long long), st_));
     const Step& s0 = prog_.steps[0];
-    const uint64_t R = re > rb ? re - rb : 0;
     // roots: inst column + next level estimate + scan temporaries
     const uint64_t per_root = 4 + 8 + 8;
     uint64_t chunk = std::max<uint64_t>(1, Budget(0) / per_root);
     chunk = std::min<uint64_t>(chunk, 0x7fffffffULL);
-    // roots rb, rb+stride, ... < re in chunks of `chunk` roots
-    const uint64_t nroots = R == 0 ? 0 : (R + stride - 1) / stride;
+    // the task's roots in chunks of `chunk` roots
+    const uint64_t nroots = task.Count();
     for (uint64_t i0 = 0; i0 < nroots; i0 += chunk) {
       uint32_t P = (uint32_t)std::min<uint64_t>(chunk, nroots - i0);
       size_t m = A_.Mark();
       uint32_t* col = (uint32_t*)A_.Alloc((size_t)P * 4);
-      k_iota<<<Grid(P, 256), 256, 0, st_>>>(col, P, (uint32_t)(rb + i0 * stride), stride);
-      Launched();
+      if (task.list) {
+        CK(cudaMemcpyAsync(col, task.list + i0, (size_t)P * 4, cudaMemcpyHostToDevice, st_));
+        root_h2d_ += (uint64_t)P * 4;
+      } else {
+        k_iota<<<Grid(P, 256), 256, 0, st_>>>(col, P, (uint32_t)(task.begin + i0 * stride), stride);
+        Launched();
+      }
       DFront F{};
       F.P = P;
       F.inst[s0.u] = col;
@@ -1073,7 +1070,6 @@ class Executor {
       Level(1, F);
       A_.Release(m);
     }
-    (void)R;
     CK(cudaEventRecord(ev1, st_));
     unsigned long long h[8];
     CK(cudaMemcpyAsync(h, ctrl_, sizeof(h), cudaMemcpyDeviceToHost, st_));
@@ -1106,6 +1102,7 @@ class Executor {
     r.stats.kernel_ms = phase[kPhaseCompute] + phase[kPhaseComputeCount] + phase[kPhasePathCount];
     r.stats.device_ms = dev_ms;
     r.stats.hot_launches = hot_;
+    r.stats.h2d_bytes = root_h2d_;
     r.stats.elapsed_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     A_.Release(mark);
@@ -1122,7 +1119,7 @@ class Executor {
   uint64_t cap_;
   int sms_ = 148;
   unsigned long long* ctrl_ = nullptr;  // [0] count [1] bytes [2] emitted [3] error flags
-  uint64_t launches_ = 0, batches_ = 0, paths_ = 0, hot_ = 0;
+  uint64_t launches_ = 0, batches_ = 0, paths_ = 0, hot_ = 0, root_h2d_ = 0;
   const uint32_t* ext_cols_ = nullptr;
   uint64_t ext_bytes_ = 0;
 
@@ -1520,15 +1517,18 @@ class Executor {
 
 }  // namespace
 
-RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx, uint64_t rb,
-                     uint64_t re, uint32_t* d_out, uint64_t cap, int tuning, uint32_t stride) {
+RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx, const RootTask& task,
+                     uint32_t* d_out, uint64_t cap, int tuning) {
   CK(cudaSetDevice(ctx.device));
-  if (re > g.n) re = g.n;
-  if (rb > re) rb = re;
+  RootTask t = task;
+  if (!t.list) {
+    if (t.end > g.n) t.end = g.n;
+    if (t.begin > t.end) t.begin = t.end;
+  }
   Executor ex(prog, g, ctx, d_out, cap);
   ex.gran_ = tuning & 0xff;
   ex.use_bitmaps_ = !(tuning & 0x100);
-  return ex.Run(rb, re, stride);
+  return ex.Run(t);
 }
 
 // EXTERNAL_GPU: the graph stays in host memory.
@@ -1539,12 +1539,15 @@ RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& c
 //              src/gpu/impl/light/ext/EXTLIGHTGPUProcessor.cuh:20-90).
 //   EXT_UMA    the adjacency lists live in managed memory and migrate on
 //              demand (EXTUMALIGHTGPUComp, src/gpu/impl/light/ext/uma/).
-RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceContext& ctx, uint64_t rb,
-                             uint64_t re, int ext_variant, uint64_t graph_budget_bytes, uint32_t stride) {
+RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceContext& ctx, const RootTask& task,
+                             int ext_variant, uint64_t graph_budget_bytes) {
   (void)graph_budget_bytes;
   CK(cudaSetDevice(ctx.device));
-  if (re > hg.n) re = hg.n;
-  if (rb > re) rb = re;
+  RootTask t = task;
+  if (!t.list) {
+    if (t.end > hg.n) t.end = hg.n;
+    if (t.begin > t.end) t.begin = t.end;
+  }
   DeviceGraph dg;
   dg.device = ctx.device;
   dg.n = hg.n;
@@ -1561,7 +1564,7 @@ RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceCon
       if (hg.m) std::memcpy(managed, hg.cols, hg.m * sizeof(uintV));
       dg.cols = managed;
       Executor ex(prog, dg, ctx, nullptr, 0);
-      r = ex.Run(rb, re, stride);
+      r = ex.Run(t);
       h2d += hg.m * sizeof(uintV);
     } else {
       const uint32_t* dcols = nullptr;
@@ -1578,7 +1581,7 @@ RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceCon
       }
       Executor ex(prog, dg, ctx, nullptr, 0);
       ex.SetExternal(dcols);
-      r = ex.Run(rb, re, stride);
+      r = ex.Run(t);
       h2d += ex.ext_h2d_bytes();
     }
   } catch (...) {
@@ -1591,7 +1594,7 @@ RunResult RunProgramExternal(const Program& prog, const HostGraph& hg, DeviceCon
   if (registered) cudaHostUnregister(hg.cols);
   if (managed) cudaFree(managed);
   cudaFree(dg.row_ptrs);
-  r.stats.h2d_bytes = h2d;
+  r.stats.h2d_bytes += h2d;
   return r;
 }
 

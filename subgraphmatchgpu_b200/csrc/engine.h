@@ -53,26 +53,42 @@ DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, ui
 DeviceGraph* UploadGraphToArena(const HostGraph& g, DeviceContext& ctx, uint64_t* h2d_bytes);
 void FreeDeviceGraph(DeviceGraph* d);
 
+// The first-level vertices of one run (an IntraPartScheduler task,
+// src/gpu/task/IntraPartScheduler.h:77-101, generalised): the roots
+// begin, begin+stride, ... < end, or, when `list` is set, exactly
+// list[0 .. list_len) in that order (host memory, ids below n).
+struct RootTask {
+  uint64_t begin = 0, end = 0;
+  uint32_t stride = 1;
+  const uint32_t* list = nullptr;
+  uint64_t list_len = 0;
+  uint64_t Count() const {
+    if (list) return list_len;
+    const uint64_t st = stride ? stride : 1;
+    return end > begin ? (end - begin + st - 1) / st : 0;
+  }
+};
+// The task of `o` on a graph of n vertices (validated: list ids below n).
+RootTask TaskOf(const sme_opts& o, uint64_t n);
+
 struct RunResult {
   uint64_t count = 0;
   uint64_t emitted = 0;
   sme_stats stats{};
 };
 
-// Runs `prog` over the root range [root_begin, root_end) of `g`.  When
-// prog.enumerate, instances are written to out (device) up to cap.
-RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx,
-                     uint64_t root_begin, uint64_t root_end, uint32_t* d_out, uint64_t cap,
-                     int tuning, uint32_t root_stride = 1);
+// Runs `prog` over the roots of `task` on `g`.  When prog.enumerate,
+// instances are written to out (device) up to cap.
+RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& ctx, const RootTask& task,
+                     uint32_t* d_out, uint64_t cap, int tuning);
 // `tuning`: low byte = intersection launch (0 auto: warp per path,
 // specialised; 1 warp per path generic; 2 flattened, specialised; 3 as 0 at
 // six blocks per SM); bit 8 set = no hub bitmaps.
 inline int Tuning(const sme_opts& o) { return (o.warp_granularity & 0xff) | (o.list_only ? 0x100 : 0); }
 
 // External (chunked) execution over a graph that stays in host memory.
-RunResult RunProgramExternal(const Program& prog, const HostGraph& g, DeviceContext& ctx,
-                             uint64_t root_begin, uint64_t root_end, int ext_variant,
-                             uint64_t graph_budget_bytes, uint32_t root_stride = 1);
+RunResult RunProgramExternal(const Program& prog, const HostGraph& g, DeviceContext& ctx, const RootTask& task,
+                             int ext_variant, uint64_t graph_budget_bytes);
 
 int DeviceCount();
 

@@ -32,6 +32,7 @@ struct Request {
   int32_t gid;
   sme_graph* attached;
   sme_opts opts;
+  std::shared_ptr<std::vector<uint32_t>> roots;  // copy of an explicit root task
   uint64_t est_bytes;
   double est_work;
   Clock::time_point submitted;
@@ -43,9 +44,7 @@ constexpr double kStarveMs = 500.0;
 // average degree to the power of the pattern's later levels.
 double EstimateWork(const HostGraph& g, const sme_opts& o) {
   const int k = Query(o.query_type).n;
-  const uint64_t end = o.root_end ? std::min<uint64_t>(o.root_end, g.n) : g.n;
-  const uint64_t stride = o.root_stride ? o.root_stride : 1;
-  const double roots = end > o.root_begin ? (double)((end - o.root_begin + stride - 1) / stride) : 0.0;
+  const double roots = (double)TaskOf(o, g.n).Count();
   const double davg = g.n ? (double)g.m / (double)g.n : 0.0;
   double w = roots;
   for (int i = 1; i < k; ++i) w *= std::max(1.0, davg);
@@ -131,19 +130,24 @@ struct sme_server {
         if (hg.oriented) RequireOrientable(prog, r.opts.enable_ordering != 0);
         DeviceGraph* dg = hg.dev;
         bool temp = false;
-        if (!dg || dg->device != o.device) {
-          dg = UploadGraph(hg, o.device, ctx->stream, nullptr);
-          temp = true;
-        }
-        uint64_t re = r.opts.root_end ? std::min<uint64_t>(r.opts.root_end, hg.n) : hg.n;
+        // an attached graph is uploaded into the slot's arena and released
+        // with it: no device allocation or free (a cudaFree would stall the
+        // other slots' streams)
+        const size_t graph_mark = ctx->arena.Mark();
         RunResult rr;
         try {
-          rr = RunProgram(prog, *dg, *ctx, r.opts.root_begin, re, nullptr, 0, Tuning(r.opts), r.opts.root_stride);
+          if (!dg || dg->device != o.device) {
+            dg = UploadGraphToArena(hg, *ctx, nullptr);
+            temp = true;
+          }
+          rr = RunProgram(prog, *dg, *ctx, TaskOf(r.opts, hg.n), nullptr, 0, Tuning(r.opts));
         } catch (...) {
           if (temp) FreeDeviceGraph(dg);
+          ctx->arena.Release(graph_mark);
           throw;
         }
         if (temp) FreeDeviceGraph(dg);
+        ctx->arena.Release(graph_mark);
         res.status = SME_OK;
         res.count = rr.count;
       } catch (const Error& e) {
@@ -239,6 +243,11 @@ sme_status sme_server_submit(sme_server* s, int32_t gid, sme_graph* attached, co
     r.attached = attached;
     r.opts = *opts;
     r.opts.device = s->o.device;
+    if (opts->num_roots > 0) {  // the caller's array may go away after submit
+      if (!opts->roots) Fail(SME_ERR_INVALID_ARG, "num_roots > 0 with a null roots array");
+      r.roots = std::make_shared<std::vector<uint32_t>>(opts->roots, opts->roots + opts->num_roots);
+      r.opts.roots = r.roots->data();
+    }
     r.submitted = Clock::now();
     {
       std::lock_guard<std::mutex> l(s->mu);
@@ -250,6 +259,7 @@ sme_status sme_server_submit(sme_server* s, int32_t gid, sme_graph* attached, co
       }
       const HostGraph& hg = attached ? attached->g : s->resident[gid]->g;
       Compile(r.opts, false);  // validate query / plan before queueing
+      TaskOf(r.opts, hg.n);    // and an explicit root task
       r.est_bytes = EstimateBytes(hg, r.opts.query_type);
       r.est_work = EstimateWork(hg, r.opts);
       r.id = s->next_id++;

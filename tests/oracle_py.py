@@ -32,6 +32,8 @@ def lib():
         L.oracle_wcoj_strided.restype = C.c_uint64
         L.oracle_wcoj_strided.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_uint64,
                                           C.c_uint64, C.c_int]
+        L.oracle_write_edge_text.restype = C.c_int
+        L.oracle_write_edge_text.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_char_p]
         _lib = L
     return _lib
 
@@ -61,6 +63,22 @@ def count_sample(row_ptrs, cols, q, roots, budget_s, threads=0, ordering=True):
                                     int(ordering), rt.ctypes.data, len(rt), threads, budget_s, C.byref(done),
                                     C.byref(el))
     return int(inst), int(done.value), float(el.value)
+
+
+def count_roots(row_ptrs, cols, q, roots, threads=0, ordering=True) -> int:
+    """Instances rooted at exactly the vertices of `roots` (an explicit root
+    task; a root listed twice counts twice)."""
+    inst, done, _ = count_sample(row_ptrs, cols, q, roots, 1e12, threads, ordering)
+    assert done == len(roots)
+    return inst
+
+
+def write_edge_text(u, v, path) -> None:
+    """SNAP text edge list ("u v" per line) for the reference's tools."""
+    uu = np.ascontiguousarray(u, dtype=np.uint32)
+    vv = np.ascontiguousarray(v, dtype=np.uint32)
+    if lib().oracle_write_edge_text(uu.ctypes.data, vv.ctypes.data, len(uu), path.encode()) != 0:
+        raise OSError(f"cannot write {path}")
 
 
 def enumerate_sorted(row_ptrs, cols, q, ordering=True) -> np.ndarray:

@@ -50,6 +50,8 @@ def test_noalloc_matches_regular_entry_point_twice(name, golden):
         if want_ref is not None and want_ref > COUNT_LIMIT:
             continue
         want = g.count(q)  # the existing entry point
+        if want_ref is not None:
+            assert want == want_ref, (name, q, want, want_ref)
         for _ in range(2):  # two calls in a row share (and reuse) the scratch
             st, got = count_noalloc(d_rp, d_cl, n, q)
             assert st == 0, sme.lib().sme_last_error().decode()
@@ -76,3 +78,30 @@ def test_noalloc_rejects_sizes_beyond_the_limit():
     g2 = sme.Graph.clique(6)
     d_rp2, d_cl2, n2 = device_csr(g2)
     assert count_noalloc(d_rp2, d_cl2, n2, 3) == (0, 15)
+
+
+def test_noalloc_rejects_lists_that_break_the_input_contract():
+    # K6 with one list made unsorted, one with a self loop, one with a
+    # duplicate neighbour: the sorted-list searches would count wrongly, so
+    # each is refused with INVALID_ARG before any enumeration
+    rp, cl = sme.Graph.clique(6).csr()
+    bad = []
+    c = cl.copy()
+    c[0], c[1] = c[1], c[0]
+    bad.append(c)
+    c = cl.copy()
+    c[int(rp[2])] = 2  # vertex 2 lists itself
+    bad.append(c)
+    c = cl.copy()
+    c[int(rp[3]) + 1] = c[int(rp[3])]  # duplicate neighbour in vertex 3's list
+    bad.append(c)
+    for c in bad:
+        import torch
+        d_rp = torch.from_numpy(rp.view(np.int64).copy()).cuda()
+        d_cl = torch.from_numpy(c.view(np.int32).copy()).cuda()
+        torch.cuda.synchronize()
+        st, _ = count_noalloc(d_rp, d_cl, len(rp) - 1, 0)
+        assert st == 1, sme.lib().sme_last_error().decode()
+        assert "strictly increasing" in sme.lib().sme_last_error().decode()
+    d_rp, d_cl, n = device_csr(sme.Graph.clique(6))
+    assert count_noalloc(d_rp, d_cl, n, 0) == (0, 20)
