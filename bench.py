@@ -1,43 +1,60 @@
 #!/usr/bin/env python3
 """Benchmark of the GPU subgraph-enumeration path (one JSON line on rank 0).
 
-Workload (the plain GPU path of the 4-clique / 4-cycle / diamond
-configuration): an undirected R-MAT graph, scale 20, edge factor 16,
-a/b/c/d = .57/.19/.19/.05, seeded, self loops and parallel edges removed,
-uint32 CSR; queries 4-clique (Q3), 4-cycle (Q1) and diamond (Q2) with the
-reference's symmetry-breaking constraints, counted with uint64 results by the
-LIGHT plan in IN_MEMORY_GPU mode (`patternmatchgpu -a 6 -m 1`).
+Workload: the 4-clique (Q3), 4-cycle (Q1) and diamond (Q2) counts, with the
+reference's symmetry-breaking constraints, on an undirected R-MAT graph of
+scale 20, edge factor 16, a/b/c/d = .57/.19/.19/.05, seed 20, generated here
+with numpy and passed through the reference's preprocessing (self loops and
+parallel edges dropped, dangling vertices dropped with an order-preserving
+relabel), uint32 CSR, uint64 counts.
 
-A step is one pass of the hot path over one task: the count of one query
-over one root-vertex range of the graph (an IntraPartScheduler task).  The
-steps cycle through (query, task) pairs; the sum over a full cycle is the
-complete count of every query.  `value` is instances/s with the graph
-resident in HBM, timed with CUDA events on the library's stream; `e2e` is the
-same metric through sme_count with the CSR in pinned host memory copied to the
-device in every step.
+A step is one query over one root task: a block of roots drawn from a seeded
+permutation of the vertices of degree <= 1024 (99% of the roots).  Both arms
+run the same steps in the same order:
+
+  * this engine (default arm): sme_count with the LIGHT plan on the resident
+    graph; `value` = instances / CUDA-event device time; `e2e` = the same
+    steps through sme_count with the CSR in pinned host memory copied to the
+    device in every step;
+  * the reference (`--impl reference`): the reference's own CPU_WCOJ DFS over
+    the same root blocks (oracle/_ref/ref_wcoj_task, compiled from its
+    sources) on the BIN file its own preprocess_graph wrote from the same edge
+    list, with every host thread.
+
+Hub roots (degree > 1024) are left out of the shared steps because the
+reference's per-root DFS cannot finish one in bounded time (a single hub root
+of the 4-clique runs for minutes on eight cores).  The engine's whole-graph
+counts, hubs included, are reported in `whole_graph`.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sme|reference]
 """
 import argparse
+import hashlib
 import json
 import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "instances/sec (4-clique, 4-cycle, diamond; R-MAT s20 ef16)"
 UNIT = "instances/s"
+QUERY_NAMES = {0: "triangle", 1: "4-cycle", 2: "diamond", 3: "4-clique", 4: "house", 7: "5-clique"}
+REF_TASK = os.path.join(ROOT, "oracle", "_ref", "ref_wcoj_task")
+REF_PREPROCESS = os.path.join(ROOT, "oracle", "_ref", "preprocess_graph")
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=9)
+    ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sme", choices=["sme", "reference"])
     ap.add_argument("--scale", type=int, default=20)
@@ -45,27 +62,110 @@ def parse():
     ap.add_argument("--seed", type=int, default=20)
     ap.add_argument("--queries", default="3,1,2")
     ap.add_argument("--algo", type=int, default=6)
-    ap.add_argument("--tasks", type=int, default=2, help="root-range tasks per query")
-    ap.add_argument("--q1-stride", type=int, default=1024, help="4-cycle: roots per strided task = n/stride")
-    ap.add_argument("--q1-tasks", type=int, default=3, help="4-cycle: strided tasks in the step cycle")
-    ap.add_argument("--root-end", type=int, default=0, help="restrict roots to [root_begin, root_end) (profiling)")
-    ap.add_argument("--root-begin", type=int, default=0)
+    ap.add_argument("--hub-degree", type=int, default=1024, help="roots above this degree are not in the shared steps")
+    ap.add_argument("--blocks", default="3:16384,1:512,2:8192", help="roots per step, per query")
+    ap.add_argument("--check-algo", type=int, default=4, help="second plan that recounts every timed step")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched / served measurements")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--task-roots", type=int, default=256, help="served: roots per request task")
-    ap.add_argument("--load", type=float, default=0.8, help="open-loop arrival rate / plain capacity")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--rates", default="50,500,5000", help="served: open-loop arrival rates (req/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--granularity", type=int, default=0, help="0 auto (specialised warp per path), 1 warp per path generic, 2 flattened, 3 specialised at six blocks per SM")
+    ap.add_argument("--granularity", type=int, default=0,
+                    help="0 auto (specialised warp per path), 1 warp per path generic, 2 flattened, "
+                         "3 specialised at six blocks per SM")
     ap.add_argument("--list-only", action="store_true", help="no hub bitmaps (comparison)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-s22", action="store_true", help="skip the R-MAT s22 4-clique leg")
+    ap.add_argument("--no-whole", action="store_true", help="skip the whole-graph counts")
+    ap.add_argument("--no-s22", action="store_true", help="skip the R-MAT s22 legs")
     ap.add_argument("--no-l2-flush", action="store_true", help="do not flush L2 between steps")
-    return ap.parse_args()
+    ap.add_argument("--threads", type=int, default=0, help="CPU threads (0: all)")
+    return ap.parse_args(argv)
 
 
+# ---------------------------------------------------------------- workload --
+def rmat_edges(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=20):
+    """R-MAT edge list: n * edge_factor edges, each picking one quadrant per
+    level (a top-left, b top-right, c bottom-left, d bottom-right) from one
+    uniform draw; vertex ids are the concatenated bits (no relabelling)."""
+    rng = np.random.default_rng(seed)
+    ne = (1 << scale) * edge_factor
+    u = np.zeros(ne, np.uint32)
+    v = np.zeros(ne, np.uint32)
+    ab, abc = a + b, a + b + c
+    one = np.uint32(1)
+    for _ in range(scale):
+        r = rng.random(ne)
+        u = (u << one) | (r >= ab).astype(np.uint32)
+        v = (v << one) | (((r >= a) & (r < ab)) | (r >= abc)).astype(np.uint32)
+    return u, v
+
+
+def raw_csr(u, v, n):
+    """Undirected CSR of an edge list as the reference's SNAP reader builds it
+    (both directions, lists sorted, self loops and parallel edges kept): the
+    input of the preprocessing step."""
+    keys = np.concatenate([(u.astype(np.uint64) << np.uint64(32)) | v, (v.astype(np.uint64) << np.uint64(32)) | u])
+    keys.sort()
+    src = (keys >> np.uint64(32)).astype(np.int64)
+    rp = np.zeros(n + 1, np.uint64)
+    rp[1:] = np.cumsum(np.bincount(src, minlength=n), dtype=np.uint64)
+    return rp, (keys & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+
+
+def csr_digest(rp, cl):
+    h = hashlib.sha1()
+    h.update(np.ascontiguousarray(rp, np.uint64).tobytes())
+    h.update(np.ascontiguousarray(cl, np.uint32).tobytes())
+    return h.hexdigest()[:16]
+
+
+def parse_blocks(spec):
+    return {int(k): int(v) for k, v in (x.split(":") for x in spec.split(","))}
+
+
+def make_steps(rp, args, count):
+    """The first `count` steps: step i is query qs[i % len(qs)] over block
+    i // len(qs) of that query's seeded permutation of the roots of degree
+    <= hub_degree (blocks wrap around the permutation)."""
+    qs = [int(q) for q in args.queries.split(",")]
+    blocks = parse_blocks(args.blocks)
+    deg = np.diff(np.asarray(rp, np.uint64)).astype(np.int64)
+    pool = np.flatnonzero(deg <= args.hub_degree).astype(np.uint32)
+    perms = {q: np.random.default_rng(args.seed * 1000 + q).permutation(pool) for q in qs}
+    steps = []
+    for i in range(count):
+        q = qs[i % len(qs)]
+        k = i // len(qs)
+        p, bsz = perms[q], min(blocks[q], len(pool))
+        start = (k * bsz) % max(len(p), 1)
+        idx = (start + np.arange(bsz)) % max(len(p), 1)
+        steps.append((q, np.ascontiguousarray(p[idx], np.uint32)))
+    return steps
+
+
+def config_of(args, n, m, digest):
+    blocks = parse_blocks(args.blocks)
+    qs = [int(q) for q in args.queries.split(",")]
+    return {"workload": f"R-MAT s{args.scale} ef{args.edge_factor} (a,b,c)=(.57,.19,.19) seed {args.seed}, numpy "
+                        f"generator + the reference's preprocessing: n={n} m={m} csr_sha1={digest}; queries "
+                        + ", ".join(f"Q{q} {QUERY_NAMES.get(q, q)}" for q in qs) +
+                        " with the reference's symmetry breaking; a step = one query over one block of roots "
+                        f"drawn from a seeded permutation of the roots of degree <= {args.hub_degree} (roots "
+                        "per block: " + ", ".join(f"Q{q} {blocks[q]}" for q in qs) + ")",
+            "plan": f"algo {args.algo} (6 = LIGHT), IN_MEMORY_GPU",
+            "l2": "GPU arm: L2 flushed before every step (256 MiB write, outside the timed region); "
+                  "inputs: CSR %d bytes" % (8 * (n + 1) + 4 * m),
+            "parallelism": "single GPU (replicas when N > 1)"}
+
+
+def per_query_summary(per_q):
+    return {str(q): {"name": QUERY_NAMES.get(q, str(q)), "instances": int(v[0]), "seconds": v[1],
+                     "value": (v[0] / v[1]) if v[1] > 0 else 0.0, "steps": v[2]} for q, v in sorted(per_q.items())}
+
+
+# ----------------------------------------------------------- measurement --
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -117,28 +217,179 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_graph(args):
-    import subgraphmatchgpu_b200 as sme
-    return sme.Graph.rmat(args.scale, args.edge_factor, 0.57, 0.19, 0.19, seed=args.seed)
+def reduce_over_ranks(dev_ms, instances, dist, device):
+    """Replicas: the job's time is the slowest rank's device time, its work
+    the sum of the ranks' instances (timing only; no data-path collective)."""
+    if dist is None:
+        return dev_ms, float(instances)
+    import torch
+    tmax = torch.tensor([float(dev_ms)], dtype=torch.float64, device=device)
+    tsum = torch.tensor([float(instances)], dtype=torch.float64, device=device)
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax.item()), float(tsum.item())
 
 
-def work_items(args, n):
-    """(query, root_begin, root_end, root_stride) tasks.  Queries whose full
-    count fits a few seconds (4-clique, diamond) use `tasks` contiguous root
-    ranges; the 4-cycle, whose full count at this scale takes minutes, uses
-    strided tasks (every `q1_stride`-th root from offset k), each an unbiased
-    1/q1_stride slice of the roots."""
-    qs = [int(q) for q in args.queries.split(",")]
-    end = args.root_end or n
-    beg = args.root_begin
-    items = []
-    for q in qs:
-        if q == 1 and not args.root_end:
-            items += [(q, k, end, args.q1_stride) for k in range(args.q1_tasks)]
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+# ------------------------------------------------------ the reference's CPU --
+def threads_of(args):
+    return args.threads or os.cpu_count() or 1
+
+
+def reference_tasks(bin_path, steps, threads, tmpdir):
+    """Runs the reference's CPU_WCOJ over each step's roots with the task
+    driver built from its sources; returns [(count, elapsed_ms)] per step.
+    One driver process per query (the graph loads once per query)."""
+    out = [None] * len(steps)
+    for q in sorted({s[0] for s in steps}):
+        idx = [i for i, s in enumerate(steps) if s[0] == q]
+        roots = np.concatenate([steps[i][1] for i in idx]) if idx else np.zeros(0, np.uint32)
+        rpath = os.path.join(tmpdir, f"roots_q{q}.u32")
+        roots.astype(np.uint32).tofile(rpath)
+        args, off = [], 0
+        for i in idx:
+            args.append(f"L:{off}:{len(steps[i][1])}")
+            off += len(steps[i][1])
+        r = subprocess.run([REF_TASK, "-f", bin_path, "-q", str(q), "-t", str(threads), "-r", rpath] + args,
+                           capture_output=True, text=True, check=True)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("task=")]
+        if len(lines) != len(idx):
+            raise RuntimeError(f"reference task driver printed {len(lines)} results for {len(idx)} tasks")
+        for i, ln in zip(idx, lines):
+            kv = dict(x.strip().split("=", 1) for x in ln.split(","))
+            out[i] = (int(kv["total_match_count"]), float(kv["elapsed_time"].rstrip("ms")))
+    return out
+
+
+def port_tasks(rp, cl, steps, threads):
+    """The oracle's C restatement of CPU_WCOJ over the same steps (used when
+    the reference's own driver was not built)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as O
+    out = []
+    for q, roots in steps:
+        t0 = time.perf_counter()
+        c = O.count_roots(rp, cl, q, roots, threads)
+        out.append((c, (time.perf_counter() - t0) * 1e3))
+    return out
+
+
+def reference_graph(args, tmpdir):
+    """The edge list through the reference's own preprocess_graph into its BIN
+    file; (bin path, row_ptrs, cols).  Without the reference's tools the
+    oracle's numpy restatement of the same preprocessing is used and the BIN
+    path is None."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as O
+    u, v = rmat_edges(args.scale, args.edge_factor, seed=args.seed)
+    if os.path.exists(REF_PREPROCESS) and os.path.exists(REF_TASK):
+        txt = os.path.join(tmpdir, "rmat.txt")
+        O.write_edge_text(u, v, txt)
+        subprocess.run([REF_PREPROCESS, "-f", txt, "-d", "0"], capture_output=True, text=True, check=True)
+        rp, cl = O.read_bin(txt + ".bin")
+        return txt + ".bin", rp, cl
+    rp, cl = raw_csr(u, v, 1 << args.scale)
+    return None, *O.preprocess_csr(rp, cl)
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm: the reference's own CPU_WCOJ on the host cores, the
+    same steps as the engine's arm (rank 0 only; other ranks exit)."""
+    if rank != 0:
+        return
+    threads = threads_of(args)
+    with tempfile.TemporaryDirectory() as tmp:
+        bin_path, rp, cl = reference_graph(args, tmp)
+        n, m = len(rp) - 1, len(cl)
+        steps = make_steps(rp, args, args.warmup + args.steps)
+        if bin_path:
+            res = reference_tasks(bin_path, steps, threads, tmp)
+            kind, what = "reference", ("the reference's CPU_WCOJ DFS (src/cpu/CPUWCOJ.h) compiled from its sources "
+                                       "(oracle/_ref/ref_wcoj_task) on the BIN its preprocess_graph wrote")
         else:
-            cuts = [beg + (end - beg) * i // args.tasks for i in range(args.tasks + 1)]
-            items += [(q, a, b, 1) for a, b in zip(cuts, cuts[1:])]
-    return items
+            res = port_tasks(rp, cl, steps, threads)
+            kind, what = "port", "the oracle's C restatement of CPU_WCOJ (the reference's tools were not built)"
+    timed = list(zip(steps, res))[args.warmup:]
+    inst = sum(c for _, (c, _) in timed)
+    ms = sum(t for _, (_, t) in timed)
+    per_q = {}
+    for (q, roots), (c, t) in timed:
+        e = per_q.setdefault(q, [0, 0.0, 0])
+        e[0] += c
+        e[1] += t / 1e3
+        e[2] += 1
+    value = inst / (ms / 1e3) if ms > 0 else 0.0
+    cb = {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+          "sample": f"{what}; the {args.steps} timed steps of the shared step list, {threads} OpenMP threads; "
+                    f"{inst} instances in {ms / 1e3:.2f} s"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": config_of(args, n, m, csr_digest(rp, cl)), "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "per_query": per_query_summary(per_q),
+            "step_counts": [int(c) for _, (c, _) in timed]}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- engine --
+def engine_graph(args):
+    """The same edge list through the engine's preprocessing
+    (sme_graph_preprocess, the reference's PreprocessGraph semantics)."""
+    import subgraphmatchgpu_b200 as sme
+    u, v = rmat_edges(args.scale, args.edge_factor, seed=args.seed)
+    rp, cl = raw_csr(u, v, 1 << args.scale)
+    g = sme.Graph.from_csr(rp, cl)
+    g.preprocess()
+    g.validate()
+    return g
+
+
+def cpu_baseline(args, g, steps, gpu_counts):
+    """The reference's CPU_WCOJ (or the oracle port) on the host cores over the
+    first timed step of each query: its rate, and its counts against the
+    engine's counts of the same steps."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    threads = threads_of(args)
+    first = {}
+    for i, (q, _) in enumerate(steps):
+        first.setdefault(q, i)
+    pick = sorted(first.values())
+    sub = [steps[i] for i in pick]
+    with tempfile.TemporaryDirectory() as tmp:
+        if os.path.exists(REF_TASK):
+            path = os.path.join(tmp, "g.bin")
+            g.write_bin(path)
+            res = reference_tasks(path, sub, threads, tmp)
+            kind = "reference"
+        else:
+            rp, cl = g.csr()
+            res = port_tasks(rp, cl, sub, threads)
+            kind = "port"
+    inst = sum(c for c, _ in res)
+    ms = sum(t for _, t in res)
+    per_q = {q: [c, t / 1e3, 1] for (q, _), (c, t) in zip(sub, res)}
+    return {"value": inst / (ms / 1e3) if ms > 0 else 0.0, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{'the reference CPU_WCOJ task driver' if kind == 'reference' else 'oracle port'} over the "
+                      f"first timed step of each query ({len(sub)} steps), {threads} threads",
+            "per_query": per_query_summary(per_q),
+            "counts_equal_gpu": all(int(c) == int(gpu_counts[i]) for i, (c, _) in zip(pick, res))}
 
 
 def small_graph_batch(num, seed):
@@ -162,8 +413,8 @@ def small_graph_batch(num, seed):
 
 def bench_batched(args, device):
     """Batched form vs the plain path (one sme_count per graph, graph copied
-    to the device per call) on the same small graphs."""
-    import numpy as np
+    to the device per call) on the same small graphs; every graph's count is
+    checked against the CPU oracle."""
     import subgraphmatchgpu_b200 as sme
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_py as O
@@ -184,8 +435,15 @@ def bench_batched(args, device):
     plain = [g.count(q, sme.GPU_LIGHT, device=device) for g, q in zip(gs, qs)]
     plain_s = time.perf_counter() - t0
     ok_plain = all(int(a) == int(b) for a, b in zip(plain, counts))
-    idx = list(range(0, len(gs), max(1, len(gs) // 64)))
-    ok_cpu = all(O.count(*gs[i].csr(), qs[i]) == int(counts[i]) for i in idx)
+    # every graph against the CPU oracle, graphs spread over the host threads
+    # (the oracle's ctypes calls release the GIL)
+    from concurrent.futures import ThreadPoolExecutor
+    t0 = time.perf_counter()
+    csrs = [g.csr() for g in gs]
+    with ThreadPoolExecutor(max_workers=threads_of(args)) as ex:
+        cpu = list(ex.map(lambda i: O.count(*csrs[i], qs[i], threads=1), range(len(gs))))
+    bad = [i for i in range(len(gs)) if cpu[i] != int(counts[i])]
+    cpu_s = time.perf_counter() - t0
     d = plan.describe()
     plan.close()
     return {"graphs": len(gs), "instances": total,
@@ -193,20 +451,22 @@ def bench_batched(args, device):
                         "group_threads": d["group_threads"], "block_threads": d["block_threads"],
                         "work_items": d["work_items"], "cuda_graph": True},
             "plain": {"value": total / plain_s, "unit": UNIT, "ms": plain_s * 1e3},
-            "counts_equal_plain": ok_plain, "counts_equal_cpu_sample": ok_cpu, "cpu_checked_graphs": len(idx)}
+            "counts_equal_plain": ok_plain, "counts_equal_cpu": not bad, "cpu_checked_graphs": len(gs),
+            "cpu_mismatches": bad[:8], "cpu_check_s": round(cpu_s, 2)}
 
 
 def bench_served(args, device):
-    """Served form: Poisson arrivals; each request is one pattern on a root
-    task of a resident R-MAT graph (s16/s18/s20, ef16) or on an attached
-    Erdos-Renyi graph (256..8192 vertices, degree 8).  Reports p50/p99 of
-    submit-to-result latency and instances/s, against the same requests run
-    one at a time through the plain path."""
+    """Served form: each request is one pattern on a root task of a resident
+    R-MAT graph (s16/s18/s20, ef16) or on an attached Erdos-Renyi graph
+    (256..8192 vertices, degree 8).  Closed loop (everything queued) and open
+    loops with Poisson arrivals at each rate, against the same requests run
+    one at a time through the plain path in arrival order."""
     import random
-    import numpy as np
     import subgraphmatchgpu_b200 as sme
     rnd = random.Random(5)
     resident = [sme.Graph.rmat(s, 16, seed=100 + s) for s in (16, 18, 20)]
+    for g in resident:
+        g.to_device(device)
     srv = sme.Server(slots=args.slots, device=device)
     gids = [srv.add_graph(g) for g in resident]
     pats = [0, 1, 2, 3, 4, 7]
@@ -220,9 +480,8 @@ def bench_served(args, device):
             k = rnd.randrange(3)
             n = resident[k].n
             stride = max(1, n // args.task_roots)
-            off = rnd.randrange(stride)
-            reqs.append((q, gids[k], None, off, n, stride))
-    lat_plain, inst = [], 0
+            reqs.append((q, gids[k], None, rnd.randrange(stride), n, stride))
+
     def plain_run(r):
         q, gid, att, a, b, st = r
         g = att if att is not None else resident[gid]
@@ -232,7 +491,6 @@ def bench_served(args, device):
         q, gid, att, a, b, st = r
         return srv.submit(q, gid=gid, attached=att, root_begin=a, root_end=b, root_stride=st)
 
-    # (1) closed loop: everything queued at once -> sustainable throughput
     t0 = time.perf_counter()
     plain_counts = [plain_run(r) for r in reqs]
     plain_s = time.perf_counter() - t0
@@ -240,149 +498,123 @@ def bench_served(args, device):
     t0 = time.perf_counter()
     ids = [submit(r) for r in reqs]
     closed = [srv.wait(i) for i in ids]
-    served_closed_s = time.perf_counter() - t0
-    # (2) open loop: Poisson arrivals at `load` x the plain path's capacity;
-    # plain = one query per launch in arrival order (a single FIFO server)
-    rate = args.load * len(reqs) / plain_s
-    gaps = [rnd.expovariate(rate) for _ in reqs]
+    served_s = time.perf_counter() - t0
+    same = [x[0] for x in closed] == plain_counts
 
-    def arrivals():
+    def arrivals(rate, seed):
+        gen = random.Random(seed)
         t = time.perf_counter()
-        for gp in gaps:
-            t += gp
+        for _ in reqs:
+            t += gen.expovariate(rate)
             yield t
 
-    lat_plain = []
-    for r, t_arr in zip(reqs, arrivals()):
-        while time.perf_counter() < t_arr:
-            time.sleep(0.0002)
-        plain_run(r)
-        lat_plain.append((time.perf_counter() - t_arr) * 1e3)
-    ids = []
-    for r, t_arr in zip(reqs, arrivals()):
-        while time.perf_counter() < t_arr:
-            time.sleep(0.0002)
-        ids.append(submit(r))
-    opened = [srv.wait(i) for i in ids]
-    lat = [x[1] for x in opened]
+    open_loop = []
+    for rate in [float(x) for x in args.rates.split(",")]:
+        lat_plain, t_busy = [], time.perf_counter()
+        for r, t_arr in zip(reqs, arrivals(rate, int(rate))):
+            while time.perf_counter() < t_arr:
+                time.sleep(0.0002)
+            plain_run(r)
+            lat_plain.append((time.perf_counter() - t_arr) * 1e3)
+        plain_wall = time.perf_counter() - t_busy
+        ids, t_busy = [], time.perf_counter()
+        for r, t_arr in zip(reqs, arrivals(rate, int(rate))):
+            while time.perf_counter() < t_arr:
+                time.sleep(0.0002)
+            ids.append(submit(r))
+        got = [srv.wait(i) for i in ids]
+        served_wall = time.perf_counter() - t_busy
+        same = same and [x[0] for x in got] == plain_counts
+        lat = [x[1] for x in got]
+        open_loop.append({"arrival_rate_per_s": rate,
+                          "served": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                                     "value": inst / served_wall, "unit": UNIT},
+                          "plain": {"p50_ms": float(np.percentile(lat_plain, 50)),
+                                    "p99_ms": float(np.percentile(lat_plain, 99)),
+                                    "value": inst / plain_wall, "unit": UNIT}})
     stats = srv.stats()
     srv.close()
-    same = [x[0] for x in closed] == plain_counts and [x[0] for x in opened] == plain_counts
     return {"requests": len(reqs), "slots": args.slots, "instances": inst,
-            "closed_loop": {"served": {"value": inst / served_closed_s, "unit": UNIT, "s": served_closed_s},
+            "closed_loop": {"served": {"value": inst / served_s, "unit": UNIT, "s": served_s},
                             "plain": {"value": inst / plain_s, "unit": UNIT, "s": plain_s}},
-            "open_loop": {"arrival_rate_per_s": rate, "load_vs_plain_capacity": args.load,
-                          "served": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))},
-                          "plain": {"p50_ms": float(np.percentile(lat_plain, 50)),
-                                    "p99_ms": float(np.percentile(lat_plain, 99))}},
-            "max_inflight": stats["max_inflight"],
+            "open_loop": open_loop, "max_inflight": stats["max_inflight"],
             "counts_equal_alone_and_in_mix": same}
 
 
-def bench_s22(args, device, tune, peak):
-    """R-MAT scale 22 (edge factor 16) 4-clique under the bench's plan: device
-    time and the intersection roofline, on the graph as generated and on its
-    degree-ordered orientation (same count)."""
+def leg_roofline(s, peak):
+    """Roofline of the intersection kernels of one run (sme_last_stats)."""
+    ach = s.algorithmic_bytes / (s.kernel_ms / 1e3) / 1e9 if s.kernel_ms > 0 else 0.0
+    return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+            "kernel_ms": round(s.kernel_ms, 3), "algorithmic_bytes": int(s.algorithmic_bytes),
+            "launches": int(s.hot_launches)}
+
+
+def bench_whole_graph(args, g, device, tune, peak):
+    """The engine alone on the whole configuration, hubs included: 4-clique
+    and diamond over every root, the 4-cycle over every 64th root (its full
+    count takes minutes); each count checked against the reuse plan."""
     import subgraphmatchgpu_b200 as sme
-    g = sme.Graph.rmat(22, args.edge_factor, 0.57, 0.19, 0.19, seed=22)
-    o, _ = g.degree_order(orient=True)
-    out = {"workload": f"R-MAT s22 ef{args.edge_factor} seed 22 (n={g.n}, m={g.m}), 4-clique, plan algo "
-                       f"{args.algo}, IN_MEMORY_GPU, one run each"}
-    for tag, gr in (("as_generated", g), ("degree_oriented", o)):
-        gr.to_device(device)
-        c = gr.count(3, args.algo, device=device, **tune)
+    out = {}
+    for q, stride in ((3, 1), (2, 1), (1, 64)):
+        c = g.count(q, args.algo, root_stride=stride, device=device, **tune)
         s = sme.last_stats()
-        ach = s.algorithmic_bytes / (s.kernel_ms / 1e3) / 1e9 if s.kernel_ms > 0 else 0.0
-        out[tag] = {"instances": c, "device_ms": s.device_ms, "value": c / (s.device_ms / 1e3), "unit": UNIT,
-                    "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
-                                 "frac": round(ach / peak, 4), "kernel_ms": s.kernel_ms,
-                                 "algorithmic_bytes": s.algorithmic_bytes, "launches": s.hot_launches}}
-        gr.release_device()
-    out["counts_equal"] = out["as_generated"]["instances"] == out["degree_oriented"]["instances"]
+        check = g.count(q, sme.GPU_GPSM_REUSE, root_stride=stride, device=device, **tune)
+        out[str(q)] = {"name": QUERY_NAMES[q], "roots": "all" if stride == 1 else f"every {stride}th",
+                       "instances": c, "device_ms": s.device_ms, "value": c / (s.device_ms / 1e3), "unit": UNIT,
+                       "roofline": leg_roofline(s, peak), "count_equals_reuse_plan": c == check}
+    inst = sum(v["instances"] for v in out.values())
+    ms = sum(v["device_ms"] for v in out.values())
+    out["all"] = {"instances": inst, "device_ms": ms, "value": inst / (ms / 1e3), "unit": UNIT}
     return out
 
 
-def reduce_over_ranks(dev_ms, instances, dist, device):
-    """Replicas: the job's time is the slowest rank's device time, its work
-    the sum of the ranks' instances (timing only; no data-path collective)."""
-    if dist is None:
-        return dev_ms, float(instances)
-    import torch
-    tmax = torch.tensor([float(dev_ms)], dtype=torch.float64, device=device)
-    tsum = torch.tensor([float(instances)], dtype=torch.float64, device=device)
-    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-    return float(tmax.item()), float(tsum.item())
-
-
-def load_traffic():
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            return json.load(f)
-    return None
-
-
-def peaks():
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
-
-
-def cpu_baseline(g, items, budget_s):
-    """The oracle port (C restatement of CPU_WCOJ, OpenMP, all host threads)
-    on a strided root sample of the same graph and query mix."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_py as O
-    rp, cl = g.csr()
-    n = len(rp) - 1
-    threads = os.cpu_count() or 1
-    import numpy as np
-    qs = sorted({it[0] for it in items})
-    # roots in a seeded random order (hubs and tail alike), processed until the
-    # per-query share of the budget runs out; roots cut short are discarded
-    roots = np.random.default_rng(12345).permutation(n).astype(np.uint32)
-    total_inst, total_t, done = 0, 0.0, {}
-    for q in qs:
-        inst, d, t = O.count_sample(rp, cl, q, roots, budget_s / len(qs), threads)
-        total_inst += inst
-        total_t += t
-        done[q] = d
-    return {"value": total_inst / total_t if total_t > 0 else 0.0, "unit": UNIT, "cores": threads,
-            "kind": "port",
-            "sample": f"CPU_WCOJ port, {threads} threads, roots of the same R-MAT graph in a seeded random order "
-                      f"until {budget_s / len(qs):.1f}s per query; completed roots per query {done}; "
-                      f"{total_inst} instances in {total_t:.2f}s"}, total_inst, total_t
-
-
-def run_reference(args, rank, world):
-    """CPU reference arm: the oracle port of CPU_WCOJ on the host cores."""
-    if rank != 0:
-        return
-    g = make_graph(args)
-    items = work_items(args, g.n)
-    # one calibrated sample per step; warm-up steps run the same sample
-    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
-    for _ in range(args.warmup):
-        cpu_baseline(g, items, per_step)
-    inst, t = 0, 0.0
-    for _ in range(args.steps):
-        cb, i, dt = cpu_baseline(g, items, per_step)
-        inst += i
-        t += dt
-    cb["value"] = inst / t if t > 0 else 0.0
-    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t / max(1, args.steps), "higher_is_better": True,
-            "scaling": "weak",
-            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": f"R-MAT s{args.scale} ef{args.edge_factor} seed {args.seed}, queries "
-                                   f"{args.queries}, CPU_WCOJ on host cores (bounded sample)"},
-            "impl": "reference", "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+def bench_s22(args, device, tune, peak):
+    """R-MAT scale 22, edge factor 16: the 4-clique on the degree-ordered
+    orientation (whole graph), the 5-clique (LIGHT and reuse plans, every
+    16th root, oriented), the house (LIGHT, a block of roots) and the
+    external mode with a device budget below the CSR size."""
+    import subgraphmatchgpu_b200 as sme
+    g = sme.Graph.rmat(22, args.edge_factor, 0.57, 0.19, 0.19, seed=22)
+    o, _ = g.degree_order(orient=True)
+    n, m, _ = g.info()
+    out = {"workload": f"R-MAT s22 ef{args.edge_factor} seed 22 (libsme generator; n={n}, m={m}); cliques on "
+                       "the degree-ordered orientation"}
+    o.to_device(device)
+    c = o.count(3, args.algo, device=device, **tune)
+    s = sme.last_stats()
+    out["4clique_oriented"] = {"instances": c, "device_ms": s.device_ms, "value": c / (s.device_ms / 1e3),
+                               "unit": UNIT, "roofline": leg_roofline(s, peak)}
+    r5 = {}
+    for algo in (sme.GPU_LIGHT, sme.GPU_GPSM_REUSE):
+        c = o.count(7, algo, root_stride=16, device=device, **tune)
+        s = sme.last_stats()
+        r5[str(algo)] = {"instances": c, "device_ms": s.device_ms, "value": c / (s.device_ms / 1e3), "unit": UNIT,
+                         "roofline": leg_roofline(s, peak)}
+    r5["counts_equal"] = r5["6"]["instances"] == r5["5"]["instances"]
+    r5["roots"] = "every 16th"
+    out["5clique_oriented"] = r5
+    o.release_device()
+    g.to_device(device)
+    deg = np.diff(g.csr()[0]).astype(np.int64)
+    roots = np.random.default_rng(22).permutation(np.flatnonzero(deg <= args.hub_degree))[:4096].astype(np.uint32)
+    hl = g.count(4, sme.GPU_LIGHT, roots=roots, device=device, **tune)
+    s = sme.last_stats()
+    hr = g.count(4, sme.GPU_GPSM_REUSE, roots=roots, device=device, **tune)
+    out["house"] = {"roots": f"4096 random roots of degree <= {args.hub_degree}", "instances": hl,
+                    "device_ms": s.device_ms, "value": hl / (s.device_ms / 1e3), "unit": UNIT,
+                    "roofline": leg_roofline(s, peak), "count_equals_reuse_plan": hl == hr}
+    g.release_device()
+    csr_bytes = 8 * (o.n + 1) + 4 * o.m
+    budget = 128 << 20
+    t0 = time.perf_counter()
+    ce = o.count(3, sme.GPU_LIGHT, mode=sme.EXTERNAL_GPU, mem_limit_bytes=budget, device=device)
+    wall = time.perf_counter() - t0
+    s = sme.last_stats()
+    out["external_4clique_oriented"] = {
+        "mem_limit_bytes": budget, "csr_bytes": csr_bytes, "instances": ce, "wall_s": wall,
+        "value": ce / wall, "unit": UNIT, "h2d_bytes": int(s.h2d_bytes), "batches": int(s.batches),
+        "count_equals_in_memory": ce == out["4clique_oriented"]["instances"]}
+    return out
 
 
 def main():
@@ -402,10 +634,12 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    g = make_graph(args)
+    g = engine_graph(args)
     n, m, dmax = g.info()
+    rp, cl = g.csr()
+    digest = csr_digest(rp, cl)
     g.to_device(local)
-    items = work_items(args, n)
+    steps = make_steps(rp, args, args.warmup + args.steps)
     tune = {"warp_granularity": args.granularity, "list_only": int(args.list_only)}
 
     # L2 (126 MB) is flushed before every step by writing a 256 MiB buffer, so
@@ -417,10 +651,10 @@ def main():
             flush_buf.fill_(1)
         torch.cuda.synchronize()
 
-    def step(i):
-        q, a, b, st = items[i % len(items)]
+    def step(i, gr=g):
+        q, roots = steps[i]
         flush_l2()
-        c = g.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
+        c = gr.count(q, args.algo, roots=roots, device=local, **tune)
         return c, sme.last_stats()
 
     for i in range(args.warmup):
@@ -432,47 +666,55 @@ def main():
     clocks.start()
     torch.cuda.synchronize()
     total_inst, dev_ms, kern_ms, alg_bytes, hot, launches = 0, 0.0, 0.0, 0, 0, 0
-    per_query = {}
-    for i in range(args.steps):
-        c, s = step(args.warmup + i)
+    per_q, counts = {}, {}
+    for i in range(args.warmup, args.warmup + args.steps):
+        c, s = step(i)
+        counts[i] = c
         total_inst += c
         dev_ms += s.device_ms
         kern_ms += s.kernel_ms
         alg_bytes += s.algorithmic_bytes
         hot += s.hot_launches
         launches += s.kernel_launches
-        q = items[(args.warmup + i) % len(items)][0]
-        per_query.setdefault(q, [0, 0.0, [0.0] * 8])
-        per_query[q][0] += c
-        per_query[q][1] += s.device_ms
-        for k in range(8):
-            per_query[q][2][k] += s.phase_ms[k]
+        e = per_q.setdefault(steps[i][0], [0, 0.0, 0])
+        e[0] += c
+        e[1] += s.device_ms / 1e3
+        e[2] += 1
     torch.cuda.synchronize()
     clk = clocks.stop()
     dev_ms_max, inst_all = reduce_over_ranks(dev_ms, total_inst, dist, "cuda")
     value = inst_all / (dev_ms_max / 1e3)
 
+    # every timed step recounted by a second plan, outside the timed region
+    check = {"plan": f"algo {args.check_algo}", "steps": 0, "equal": True}
+    for i in counts:
+        q, roots = steps[i]
+        c2 = g.count(q, args.check_algo, roots=roots, device=local)
+        check["steps"] += 1
+        check["equal"] = check["equal"] and c2 == counts[i]
+
     # end to end through the C-ABI: CSR in pinned host memory, copied every step
     e2e = None
     if not args.no_e2e:
-        rp, cl = g.csr()
         prp = torch.from_numpy(rp).pin_memory()
         pcl = torch.from_numpy(cl).pin_memory()
         gh = sme.Graph.from_csr(prp.numpy(), pcl.numpy(), copy=False)
         e_inst, e_t, h2d, d2h = 0, 0.0, 0, 0
-        q, a, b, st = items[-1]
-        gh.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
-        for i in range(args.steps):
-            q, a, b, st = items[(args.warmup + i) % len(items)]
+        q, roots = steps[0]
+        gh.count(q, args.algo, roots=roots, device=local, **tune)
+        for i in range(args.warmup, args.warmup + args.steps):
+            q, roots = steps[i]
             flush_l2()
             t0 = time.perf_counter()
-            e_inst += gh.count(q, args.algo, root_begin=a, root_end=b, root_stride=st, device=local, **tune)
+            e_inst += gh.count(q, args.algo, roots=roots, device=local, **tune)
             e_t += time.perf_counter() - t0
             s = sme.last_stats()
             h2d += s.h2d_bytes
             d2h += s.d2h_bytes
         e2e = {"value": e_inst * world / e_t, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
-               "d2h_bytes_per_step": d2h // args.steps}
+               "d2h_bytes_per_step": d2h // args.steps,
+               "note": "wall clock around each sme_count; the CSR is uploaded from pinned host memory into the "
+                       "call's arena, the step's root list copied with it and the count read back"}
         del gh
 
     peak, peak_kind = peaks()
@@ -485,53 +727,49 @@ def main():
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
                 "kernel": "intersection kernels (COMPUTE / COMPUTE_COUNT / COMPUTE_PATH_COUNT)",
-                "algorithmic_bytes_per_launch": alg_per_launch,
-                "avg_launch_ms": kern_ms / max(hot, 1),
+                "algorithmic_bytes_per_launch": alg_per_launch, "avg_launch_ms": kern_ms / max(hot, 1),
+                "bytes_definition": "per path: 12 per backward list (row pointers + gathered vertex) + 4 x clipped "
+                                    "pivot length x lists intersected + 4 per candidate written",
                 "traffic": traffic,
                 "dram_achieved_gbs": (round(traffic / (kern_ms / max(hot, 1) / 1e3) / 1e9, 1)
                                       if traffic and kern_ms > 0 else None),
-                "traffic_source": tr.get("source") if tr else None,
-                "note": "algorithmic bytes count every referenced adjacency list in full (merge bound); hub "
-                        "lists are answered from dense bitmaps and L2, so achieved/peak exceeds 1 while DRAM "
-                        "traffic stays far below it: the kernels are L2-latency bound"}
+                "traffic_source": tr.get("source") if tr else None}
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb, _, _ = cpu_baseline(g, items, args.cpu_seconds)
-    forms = None
-    if rank == 0 and world == 1 and not args.no_forms:
-        forms = {}
-        for name, fn in (("batched", bench_batched), ("served", bench_served)):
-            try:
-                forms[name] = fn(args, local)
-            except Exception as e:  # reported in the line, never dropped silently
-                forms[name] = {"error": f"{type(e).__name__}: {e}"}
-    s22 = None
-    if rank == 0 and world == 1 and not args.no_s22:
+        timed_steps = [steps[i] for i in range(args.warmup, args.warmup + args.steps)]
         try:
-            s22 = bench_s22(args, local, tune, peak)
-        except Exception as e:
-            s22 = {"error": f"{type(e).__name__}: {e}"}
+            cb = cpu_baseline(args, g, timed_steps, [counts[i] for i in range(args.warmup, args.warmup + args.steps)])
+            cb["per_query_ratio"] = {q: (per_query_summary(per_q)[q]["value"] / v["value"] if v["value"] else None)
+                                     for q, v in cb["per_query"].items()}
+        except Exception as ex:  # reported in the line, never dropped silently
+            cb = {"error": f"{type(ex).__name__}: {ex}"}
+    legs = {}
+    if rank == 0 and world == 1:
+        if not args.no_whole:
+            legs["whole_graph"] = bench_whole_graph(args, g, local, tune, peak)
+        g.release_device()
+        if not args.no_forms:
+            for name, fn in (("batched", bench_batched), ("served", bench_served)):
+                try:
+                    legs[name] = fn(args, local)
+                except Exception as ex:
+                    legs[name] = {"error": f"{type(ex).__name__}: {ex}"}
+        if not args.no_s22:
+            try:
+                legs["s22"] = bench_s22(args, local, tune, peak)
+            except Exception as ex:
+                legs["s22"] = {"error": f"{type(ex).__name__}: {ex}"}
 
     if rank == 0:
+        cfg = config_of(args, n, m, digest)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": f"R-MAT s{args.scale} ef{args.edge_factor} (a,b,c)=(.57,.19,.19) seed "
-                                   f"{args.seed}: n={n} m={m} max_degree={dmax}; queries {args.queries} "
-                                   f"(Q3 4-clique, Q1 4-cycle, Q2 diamond), plan algo {args.algo} "
-                                   f"(6=LIGHT), IN_MEMORY_GPU; tasks: {args.tasks} root ranges per query, "
-                                   f"4-cycle {args.q1_tasks} strided tasks of every {args.q1_stride}-th root",
-                       "l2": ("L2 flushed before every step (256 MiB write, outside the timed region); "
-                              if not args.no_l2_flush else "no L2 flush; ") +
-                             "CSR bytes %d" % (8 * (n + 1) + 4 * m),
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "per_query": {str(q): {"instances": v[0], "device_ms": v[1],
-                                              "phase_ms": dict(zip(sme.Stats.PHASES, [round(x, 3) for x in v[2]]))}
-                                     for q, v in per_query.items()}},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
-            "gpu_launches": launches, "forms": forms, "s22_4clique": s22,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": cfg,
+            "per_query": per_query_summary(per_q), "counts_checked": check,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk, "gpu_launches": launches,
+            "step_counts": [int(counts[i]) for i in sorted(counts)], "max_degree": dmax, **legs,
         }
         print(json.dumps(line), flush=True)
     if dist:

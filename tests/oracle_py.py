@@ -73,6 +73,24 @@ def count_roots(row_ptrs, cols, q, roots, threads=0, ordering=True) -> int:
     return inst
 
 
+def preprocess_csr(row_ptrs, cols):
+    """PreprocessGraph::Preprocess (src/preprocess/PreprocessGraph.h:13-95) in
+    numpy: drop self loops and repeated neighbours of sorted lists, then the
+    vertices left without edges, relabelling the rest densely in id order."""
+    rp = np.asarray(row_ptrs, np.uint64).astype(np.int64)
+    cl = np.asarray(cols, np.uint32)
+    n = len(rp) - 1
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
+    keep = cl.astype(np.int64) != src
+    keep[1:] &= ~((cl[1:] == cl[:-1]) & (src[1:] == src[:-1]))
+    src, dst = src[keep], cl[keep].astype(np.int64)
+    deg = np.bincount(src, minlength=n)
+    new_id = np.cumsum(deg > 0) - 1
+    nrp = np.zeros(int((deg > 0).sum()) + 1, np.uint64)
+    nrp[1:] = np.cumsum(deg[deg > 0])
+    return nrp, new_id[dst].astype(np.uint32)
+
+
 def write_edge_text(u, v, path) -> None:
     """SNAP text edge list ("u v" per line) for the reference's tools."""
     uu = np.ascontiguousarray(u, dtype=np.uint32)
