@@ -594,40 +594,134 @@ void TransformIndexBased(VertexReusePlan& vp, const SearchSequence& seq) {
   for (auto& x : vp.separate) x = otn[x];
 }
 
-// Reuse of the intersection cached at `source` (index based) with conn
-// `conn`, identity mapping on 0..source-1 and source -> target.
-ReuseConnMeta AncestorMeta(std::vector<uintV> conn, uintV source, uintV target, size_t n) {
+// One reuse meta of a hard-coded plan: the intersection over `source_conn`
+// cached at level `source` is reused as the intersection over `conn` here;
+// `pairs` map source-side pattern vertices to this side (the rest map to n).
+// Index based, as the reference's hard-coded plans are.
+struct HardMeta {
+  std::vector<uintV> conn, source_conn;
+  uintV source;
+  std::vector<std::pair<uintV, uintV>> pairs;
+};
+struct HardLevel {
+  std::vector<uintV> separate;
+  std::vector<HardMeta> reuse;
+};
+struct HardPlan {
+  std::vector<uintV> seq;
+  std::vector<HardLevel> levels;  // levels 1..n-1 (level 0 has nothing)
+};
+
+ReuseConnMeta MakeMeta(const HardMeta& h, size_t n) {
   ReuseConnMeta r;
-  r.conn = conn;
-  r.source_conn = conn;
-  r.source_vertex = source;
+  r.conn = h.conn;
+  r.source_conn = h.source_conn;
+  r.source_vertex = h.source;
   r.mapping.assign(n, (uintV)n);
-  for (uintV u = 0; u < source; ++u) r.mapping[u] = u;
-  r.mapping[source] = target;
+  for (auto& pr : h.pairs) r.mapping[pr.first] = pr.second;
+  std::sort(r.conn.begin(), r.conn.end());
+  std::sort(r.source_conn.begin(), r.source_conn.end());
   return r;
+}
+
+// The plans GPU_GPSM_REUSE runs by default (ReuseTraversalPlanHardcode::
+// Generate, src/query/optimizer/ReuseTraversalPlanHardCode.h:9-72): Q0
+// :74-84, Q2 :86-110, Q3 :112-132, Q5 (its Auto variant) :178-218, Q6
+// :220-255, Q7 :257-282, Q8 :284-310, Q9 :346-375, Q10 :434-468, Q11
+// :523-556, Q12 (Auto) :583-612, Q13 (Auto) :669-705.  The level shape is
+// the same in every plan: level 1 intersects {0}, level 2 {0, 1}, and the
+// cliques chain the previous level's cache.  Q1 and Q4 have none (the
+// reference asserts).
+bool HardcodedPlan(int t, size_t n, HardPlan& hp) {
+  using P = std::pair<uintV, uintV>;
+  auto ancestor = [](std::vector<uintV> conn, uintV source, uintV target) {
+    HardMeta m{conn, conn, source, {}};
+    for (uintV u = 0; u < source; ++u) m.pairs.push_back(P(u, u));
+    m.pairs.push_back(P(source, target));
+    return m;
+  };
+  auto mapped = [](std::vector<uintV> conn, uintV source, std::vector<P> pairs) {
+    return HardMeta{conn, {0, 1}, source, pairs};
+  };
+  hp.seq.resize(n);
+  for (size_t i = 0; i < n; ++i) hp.seq[i] = (uintV)i;
+  hp.levels.assign(n, HardLevel());
+  if (n > 1) hp.levels[1].separate = {0};
+  if (n > 2) hp.levels[2].separate = {0, 1};
+  switch (t) {
+    case 0:
+      return true;
+    case 2:
+      hp.seq = {0, 2, 1, 3};
+      hp.levels[3].reuse = {ancestor({0, 1}, 2, 3)};
+      return true;
+    case 3:
+    case 7:
+    case 11:
+      for (size_t k = 3; k < n; ++k) {
+        std::vector<uintV> c;
+        for (uintV x = 0; x + 1 < k; ++x) c.push_back(x);
+        hp.levels[k].reuse = {ancestor(c, (uintV)(k - 1), (uintV)k)};
+        hp.levels[k].separate = {(uintV)(k - 1)};
+      }
+      return true;
+    case 5:
+      hp.seq = {0, 2, 3, 4, 5, 1};
+      hp.levels[3].reuse = {mapped({0, 2}, 2, {P(0, 0), P(1, 2), P(2, 3)})};
+      hp.levels[4].reuse = {mapped({0, 3}, 2, {P(0, 0), P(1, 3), P(2, 4)})};
+      hp.levels[5].reuse = {ancestor({0, 1}, 2, 5)};
+      return true;
+    case 6:
+      hp.seq = {0, 3, 1, 2, 4};
+      hp.levels[3].reuse = {ancestor({0, 1}, 2, 3)};
+      hp.levels[3].separate = {2};
+      hp.levels[4].reuse = {ancestor({0, 1}, 2, 4)};
+      return true;
+    case 8:
+      hp.levels[3].reuse = {ancestor({0, 1}, 2, 3)};
+      hp.levels[4].separate = {2, 3};
+      return true;
+    case 9:
+      hp.levels[3].reuse = {ancestor({0, 1}, 2, 3)};
+      hp.levels[4].reuse = {mapped({0, 2}, 2, {P(0, 0), P(1, 2), P(2, 4)})};
+      return true;
+    case 10:
+      hp.seq = {0, 1, 2, 4, 3};
+      hp.levels[3].reuse = {ancestor({0, 1}, 2, 3)};
+      hp.levels[4].reuse = {mapped({0, 3}, 2, {P(0, 0), P(1, 3), P(2, 4)})};
+      hp.levels[4].separate = {2};
+      return true;
+    case 12:
+      hp.seq = {0, 1, 3, 2, 4};
+      hp.levels[3].reuse = {ancestor({0, 1}, 2, 3)};
+      hp.levels[3].separate = {2};
+      hp.levels[4].reuse = {ancestor({0, 1, 2}, 3, 4)};
+      return true;
+    case 13:
+      hp.seq = {0, 1, 2, 5, 4, 3};
+      hp.levels[3].reuse = {mapped({0, 2}, 2, {P(0, 0), P(1, 2), P(2, 3)})};
+      hp.levels[4].reuse = {mapped({1, 2}, 2, {P(0, 1), P(1, 2), P(2, 4)})};
+      hp.levels[5].reuse = {ancestor({0, 1}, 2, 5)};
+      return true;
+    default:
+      return false;
+  }
 }
 }  // namespace
 
-bool HasHardcodedReusePlan(int t) { return t == 0 || t == 2 || t == 3 || t == 7 || t == 11; }
+bool HasHardcodedReusePlan(int t) {
+  HardPlan hp;
+  return HardcodedPlan(t, 6, hp);
+}
 
-// Hard-coded reuse plans (ReuseTraversalPlanHardCode.h:74-132, :257-282,
-// :523-556); index based.
 static void HardcodedReuse(int t, size_t n, SearchSequence& seq, std::vector<VertexReusePlan>& lv) {
-  seq.resize(n);
-  for (size_t i = 0; i < n; ++i) seq[i] = (uintV)i;
+  HardPlan hp;
+  HardcodedPlan(t, n, hp);
+  seq.assign(hp.seq.begin(), hp.seq.end());
   lv.assign(n, VertexReusePlan());
-  if (t == 2) seq = {0, 2, 1, 3};
-  lv[1].separate = {0};
-  if (n > 2) lv[2].separate = {0, 1};
-  if (t == 2) {
-    lv[3].reuse.push_back(AncestorMeta({0, 1}, 2, 3, n));
-  } else if (t == 3 || t == 7 || t == 11) {
-    for (size_t k = 3; k < n; ++k) {
-      std::vector<uintV> c;
-      for (uintV x = 0; x + 1 < k; ++x) c.push_back(x);
-      lv[k].reuse.push_back(AncestorMeta(c, (uintV)(k - 1), (uintV)k, n));
-      lv[k].separate = {(uintV)(k - 1)};
-    }
+  for (size_t k = 0; k < n; ++k) {
+    lv[k].separate.assign(hp.levels[k].separate.begin(), hp.levels[k].separate.end());
+    for (auto& h : hp.levels[k].reuse) lv[k].reuse.push_back(MakeMeta(h, n));
   }
 }
 
@@ -700,6 +794,13 @@ std::string ReusePlan::Describe() const {
     }
     os << (cache_required[i] ? "  (cached)" : "") << "\n";
   }
+  // each reuse meta's vertex mapping (source side -> this side; n = none)
+  for (size_t i = 0; i < levels.size(); ++i)
+    for (auto& r : levels[i].reuse) {
+      os << "mapping level " << i << ":";
+      for (auto x : r.mapping) os << " " << x;
+      os << "\n";
+    }
   return os.str();
 }
 

@@ -6,7 +6,10 @@ has the reference sources; the outputs are committed).
                  CPU program `patternmatchcpu -a 0` (CPU_WCOJ), built from the
                  reference sources by oracle/Makefile into oracle/_ref/
 * plans/*.txt    the reference's own `test_plan` output (LIGHT plan with
-                 NON_MATERIALIZE_OPT, reuse plan with autogen) per query
+                 NON_MATERIALIZE_OPT, reuse plan with autogen) per query, and
+                 (q*_reuse_hardcoded.txt) the hard-coded reuse plan that
+                 `patternmatchgpu -a 5` runs, printed with its vertex mappings
+                 by oracle/_ref/ref_reuse_plan
 * preprocess.json  SHA-256 of the BIN file the reference's `preprocess_graph`
                  writes for a messy SNAP edge list, and of libsme's result for
                  the same text (they must be identical)
@@ -15,8 +18,9 @@ has the reference sources; the outputs are committed).
                  edge list, and as BIN for an edge list with large, zero-padded
                  vertex names read through its .lvid reader (messy.lvid)
 
-Usage:  python tests/golden/make_golden.py [formats]   (after `make -C oracle ref`;
-        `formats` regenerates formats.json and messy.lvid only)
+Usage:  python tests/golden/make_golden.py [formats|hardcoded]   (after
+        `make -C oracle ref`; `formats` regenerates formats.json and messy.lvid
+        only, `hardcoded` the hard-coded reuse plans only)
 """
 import hashlib
 import json
@@ -167,9 +171,25 @@ def formats():
     print("formats", res)
 
 
+# queries with a hard-coded reuse plan (Q1 and Q4 end in the reference's assert)
+HARDCODED = (0, 2, 3, 5, 6, 7, 8, 9, 10, 11, 12, 13)
+
+
+def hardcoded():
+    os.makedirs(os.path.join(HERE, "plans"), exist_ok=True)
+    for q in HARDCODED:
+        out = subprocess.run([os.path.join(REF, "ref_reuse_plan"), str(q)], capture_output=True, text=True,
+                             check=True).stdout
+        with open(os.path.join(HERE, "plans", f"q{q}_reuse_hardcoded.txt"), "w") as f:
+            f.write(out)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["formats"]:
         formats()
+    elif sys.argv[1:] == ["hardcoded"]:
+        hardcoded()
     else:
         main()
         formats()
+        hardcoded()

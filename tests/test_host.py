@@ -109,13 +109,29 @@ def test_reuse_autogen_plan_matches_reference_test_plan(q):
     assert rl == ml
 
 
+HARDCODED = (0, 2, 3, 5, 6, 7, 8, 9, 10, 11, 12, 13)
+
+
+@pytest.mark.parametrize("q", HARDCODED)
+def test_hardcoded_reuse_plan_matches_reference(q):
+    # the plan `patternmatchgpu -a 5` runs: search sequence, per-level reuse
+    # metas and separate lists, and every meta's vertex mapping
+    ref = open(os.path.join(ROOT, "tests", "golden", "plans", f"q{q}_reuse_hardcoded.txt")).read().splitlines()
+    mine = sme.plan_describe(q, 3).splitlines()
+    rl = [l for l in ref if l.startswith(("level ", "mapping level "))]
+    ml = [l.split("  (cached)")[0] for l in mine if l.startswith(("level ", "mapping level "))]
+    assert rl == ml
+    seq = next(l for l in ref if l.startswith("search sequence for intra-partition:")).split(":")[1].split()
+    assert mine[0].split("search sequence:")[1].split() == seq
+
+
 def test_special_plans_and_hardcoded_reuse():
     # COMPRESS_LEVEL_SPECIAL (LazyTraversalPlanGenerator.h:244-300)
     q2 = sme.plan_describe(2, 4)
     assert "(COMPUTE_PATH_COUNT,1),(COMPUTE_PATH_COUNT,3),(COUNT,4)" in q2
     assert "(COUNT,6)" in sme.plan_describe(5, 4)
-    # hard-coded reuse plans exist for Q0,Q2,Q3,Q7,Q11; Q1/Q4 have none
-    for q in (0, 2, 3, 7, 11):
+    # hard-coded reuse plans exist for every query but Q1/Q4
+    for q in HARDCODED:
         sme.plan_describe(q, 3)
     for q in (1, 4):
         with pytest.raises(sme.SmeError) as e:
