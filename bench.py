@@ -572,48 +572,77 @@ def bench_s22(args, device, tune, peak):
     """R-MAT scale 22, edge factor 16: the 4-clique on the degree-ordered
     orientation (whole graph), the 5-clique (LIGHT and reuse plans, every
     16th root, oriented), the house (LIGHT, a block of roots) and the
-    external mode with a device budget below the CSR size."""
+    external mode with a device budget below the CSR size.  Each leg reports
+    its own error instead of ending the others."""
     import subgraphmatchgpu_b200 as sme
     g = sme.Graph.rmat(22, args.edge_factor, 0.57, 0.19, 0.19, seed=22)
     o, _ = g.degree_order(orient=True)
     n, m, _ = g.info()
     out = {"workload": f"R-MAT s22 ef{args.edge_factor} seed 22 (libsme generator; n={n}, m={m}); cliques on "
                        "the degree-ordered orientation"}
-    o.to_device(device)
-    c = o.count(3, args.algo, device=device, **tune)
-    s = sme.last_stats()
-    out["4clique_oriented"] = {"instances": c, "device_ms": s.device_ms, "value": c / (s.device_ms / 1e3),
-                               "unit": UNIT, "roofline": leg_roofline(s, peak)}
-    r5 = {}
-    for algo in (sme.GPU_LIGHT, sme.GPU_GPSM_REUSE):
-        c = o.count(7, algo, root_stride=16, device=device, **tune)
+
+    def leg(name, fn):
+        try:
+            out[name] = fn()
+        except Exception as ex:  # reported in the line, never dropped silently
+            out[name] = {"error": f"{type(ex).__name__}: {ex}"}
+
+    def run(gr, q, algo, **kw):
+        c = gr.count(q, algo, device=device, **kw)
         s = sme.last_stats()
-        r5[str(algo)] = {"instances": c, "device_ms": s.device_ms, "value": c / (s.device_ms / 1e3), "unit": UNIT,
-                         "roofline": leg_roofline(s, peak)}
-    r5["counts_equal"] = r5["6"]["instances"] == r5["5"]["instances"]
-    r5["roots"] = "every 16th"
-    out["5clique_oriented"] = r5
+        return c, {"instances": c, "device_ms": s.device_ms, "value": c / (s.device_ms / 1e3), "unit": UNIT,
+                   "roofline": leg_roofline(s, peak)}
+
+    o.to_device(device)
+    clique4 = {}
+
+    def four():
+        c, r = run(o, 3, args.algo, **tune)
+        clique4["count"] = c
+        c5, _ = run(o, 3, sme.GPU_GPSM_REUSE, **tune)
+        r["count_equals_reuse_plan"] = c == c5
+        return r
+
+    def five():
+        r5 = {"roots": "every 16th"}
+        for algo in (sme.GPU_LIGHT, sme.GPU_GPSM_REUSE):
+            _, r5[str(algo)] = run(o, 7, algo, root_stride=16, **tune)
+        r5["counts_equal"] = r5["6"]["instances"] == r5["5"]["instances"]
+        return r5
+
+    leg("4clique_oriented", four)
+    leg("5clique_oriented", five)
     o.release_device()
-    g.to_device(device)
-    deg = np.diff(g.csr()[0]).astype(np.int64)
-    roots = np.random.default_rng(22).permutation(np.flatnonzero(deg <= args.hub_degree))[:4096].astype(np.uint32)
-    hl = g.count(4, sme.GPU_LIGHT, roots=roots, device=device, **tune)
-    s = sme.last_stats()
-    hr = g.count(4, sme.GPU_GPSM_REUSE, roots=roots, device=device, **tune)
-    out["house"] = {"roots": f"4096 random roots of degree <= {args.hub_degree}", "instances": hl,
-                    "device_ms": s.device_ms, "value": hl / (s.device_ms / 1e3), "unit": UNIT,
-                    "roofline": leg_roofline(s, peak), "count_equals_reuse_plan": hl == hr}
-    g.release_device()
-    csr_bytes = 8 * (o.n + 1) + 4 * o.m
-    budget = 128 << 20
-    t0 = time.perf_counter()
-    ce = o.count(3, sme.GPU_LIGHT, mode=sme.EXTERNAL_GPU, mem_limit_bytes=budget, device=device)
-    wall = time.perf_counter() - t0
-    s = sme.last_stats()
-    out["external_4clique_oriented"] = {
-        "mem_limit_bytes": budget, "csr_bytes": csr_bytes, "instances": ce, "wall_s": wall,
-        "value": ce / wall, "unit": UNIT, "h2d_bytes": int(s.h2d_bytes), "batches": int(s.batches),
-        "count_equals_in_memory": ce == out["4clique_oriented"]["instances"]}
+
+    def house():
+        # the LIGHT house plan roots its tasks at pattern vertex u1 (search
+        # sequence 1 2 3 0 4): the check is the same plan with every vertex
+        # materialised (compress level 0)
+        g.to_device(device)
+        deg = np.diff(g.csr()[0]).astype(np.int64)
+        roots = np.random.default_rng(22).permutation(np.flatnonzero(deg <= args.hub_degree))[:4096]
+        roots = roots.astype(np.uint32)
+        c, r = run(g, 4, sme.GPU_LIGHT, roots=roots, **tune)
+        c0, _ = run(g, 4, sme.GPU_LIGHT, roots=roots, compress_level=0, **tune)
+        g.release_device()
+        r.update({"roots": f"4096 random roots of degree <= {args.hub_degree}",
+                  "count_equals_compress_level_0": c == c0})
+        return r
+
+    def external():
+        csr_bytes = 8 * (o.n + 1) + 4 * o.m
+        budget = 256 << 20
+        t0 = time.perf_counter()
+        ce = o.count(3, sme.GPU_LIGHT, mode=sme.EXTERNAL_GPU, mem_limit_bytes=budget, device=device)
+        wall = time.perf_counter() - t0
+        s = sme.last_stats()
+        return {"mem_limit_bytes": budget, "csr_bytes": csr_bytes, "instances": ce, "wall_s": wall,
+                "device_ms": s.device_ms, "value": ce / wall, "unit": UNIT, "h2d_bytes": int(s.h2d_bytes),
+                "batches": int(s.batches), "external_load_ms": s.phase_ms[7],
+                "count_equals_in_memory": ce == clique4.get("count")}
+
+    leg("house", house)
+    leg("external_4clique_oriented", external)
     return out
 
 

@@ -75,12 +75,18 @@ typedef struct sme_opts {
   int32_t device;          /* CUDA device ordinal                            */
   uint64_t mem_limit_bytes;/* device budget for frontiers+graph; 0 = auto    */
   uint64_t root_begin;     /* first-level vertex range [begin,end) (a task   */
-  uint64_t root_end;       /*  of IntraPartScheduler); end==0 means all      */
+  uint64_t root_end;       /*  of IntraPartScheduler); end==0 means all.
+                              The first level is the plan's first pattern
+                              vertex: u0, except in the LIGHT house plan
+                              (Q4), whose search sequence starts at u1      */
   int32_t warp_granularity;/* intersection launch shape: 0 auto (warp per
                               path, specialised on list count, tuned
                               occupancy), 1 warp per path generic,
                               2 flattened (32 paths per warp), 3 as 0 with
-                              six blocks per SM throughout                  */
+                              six blocks per SM throughout, 4 as 0 with a
+                              CTA per path whose clipped pivot is long
+                              (two-list steps; the other list staged in
+                              shared memory by a bulk copy)                 */
   int32_t list_only;       /* 1: membership by binary search only, no hub
                               bitmaps (comparison knob)                      */
   uint32_t root_stride;    /* roots are root_begin, +stride, ... < root_end

@@ -214,10 +214,13 @@ __global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __res
 // step with two or three lists keeps fewer values live; NEX = 0 is for steps
 // without `!=` conditions (no exclusion array).  The launcher guarantees
 // both bounds.
-template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV>
+// DEFER (two lists, no `!=`): a path whose clipped pivot holds at least
+// hv.min_len elements is queued for k_compute_cta instead.
+template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV, bool DEFER = false>
 __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
-    uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
+    uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err,
+    DHeavy hv) {
   const uintE* __restrict__ rp = G.rp;
   const uint32_t* __restrict__ cols = G.cols;
   const int lane = threadIdx.x & 31;
@@ -269,6 +272,15 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     BoundsT<NEX> bd = MakeBounds<NEX>(s.cond, F, p);
     uint32_t r0 = 0, r1 = 0;
     if (nl > 0) Range(L[0], N[0], bd, r0, r1);
+    if (DEFER && nl == 2 && r1 - r0 >= hv.min_len) {
+      uint32_t slot = 0;
+      if (lane == 0) slot = atomicAdd(hv.q, 1u);
+      slot = __shfl_sync(FULL, slot, 0);
+      if (slot < hv.cap) {
+        if (lane == 0) hv.q[1 + slot] = p;
+        continue;
+      }
+    }
 
     uint64_t out_off = 0;
     if (MODE == 0) {
@@ -350,6 +362,213 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     if (lane == 0 && local) atomicAdd(acc, local);
   }
   if (lane == 0 && bytes) atomicAdd(acc + 1, bytes);
+}
+
+// ---- intersection, one CTA per long-pivot path ----------------------------
+// The paths k_compute<..., DEFER> queued: two lists, no `!=` conditions, a
+// clipped pivot of at least DHeavy::min_len elements.  All CTA_THREADS
+// threads walk one path's pivot.  When the other list is not a hub (no
+// bitmap), its window between the pivot's first and last value is staged in
+// shared memory first: the 16-byte-aligned interior by one bulk copy
+// (cp.async.bulk global -> shared, completion on an mbarrier, the source this
+// GPU's own memory), the at most three elements on either ragged end by plain
+// loads; every binary search then probes shared memory instead of L2.  The
+// window is staged only when it fits `win_cap` elements and holds at most
+// kStageRatio elements per pivot element (else the copy would read more than
+// the searches).  Results equal k_compute's: MODE 0 writes the sorted set at
+// the path's offset (block-ordered compaction), MODE 1 counts (ranked into a
+// partner set when the step has one), MODE 2 stores the count.
+constexpr int CTA_THREADS = 512;
+constexpr int CTA_WARPS = CTA_THREADS / 32;
+constexpr uint32_t kStageRatio = 16;
+constexpr uint32_t kMbarSpins = 1u << 22;
+
+__device__ __forceinline__ uint32_t LowerBoundShared(const uint32_t* a, uint32_t n, uint32_t x) {
+  if (n == 0) return 0;
+  const uint32_t* base = a;
+  while (n > 1) {
+    const uint32_t half = n >> 1;
+    base = base[half] < x ? base + half : base;
+    n -= half;
+  }
+  return (uint32_t)(base - a) + (base[0] < x ? 1u : 0u);
+}
+
+__device__ __forceinline__ bool MbarTryWait(uint32_t bar, uint32_t phase) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(phase)
+      : "memory");
+  return done != 0;
+}
+
+// Waits (bounded) for the phase of `bar` to complete; false if it gave up.
+__device__ __forceinline__ bool MbarWait(uint32_t bar, uint32_t phase) {
+  for (uint32_t i = 0; i < kMbarSpins; ++i)
+    if (MbarTryWait(bar, phase)) return true;
+  return false;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(CTA_THREADS, 2) k_compute_cta(
+    DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
+    uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err,
+    const uint32_t* __restrict__ hq, uint32_t hq_cap, uint32_t win_cap) {
+  extern __shared__ __align__(128) uint32_t win[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t wtot[CTA_WARPS];
+  const uintE* __restrict__ rp = G.rp;
+  const uint32_t* __restrict__ cols = G.cols;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  uint32_t phase = 0;
+  unsigned long long local = 0, bytes = 0;
+  const uint64_t base = (MODE == 0 && b0 > 0) ? est_incl[b0 - 1] : 0;
+  const uint32_t nheavy = min(hq[0], hq_cap);
+  for (uint32_t i = blockIdx.x; i < nheavy; i += gridDim.x) {
+    const uint32_t p = hq[1 + i];
+    // the two lists (backward lists, then the reused set), pivot first
+    const uint32_t* L[2];
+    const uint32_t* Bm[2] = {nullptr, nullptr};
+    uint32_t N[2];
+    int nl = 0;
+    for (int k = 0; k < 2 && k < s.nconn; ++k) {
+      const uint32_t v = F.inst[s.conn[k]][p];
+      const uintE b = rp[v], e = rp[v + 1];
+      L[k] = cols + b;
+      N[k] = (uint32_t)(e - b);
+      Bm[k] = HubBitmap(G, v);
+      nl = k + 1;
+    }
+    if (s.reuse >= 0 && nl < 2) {
+      GetSet(F, s.reuse, p, L[nl], N[nl]);
+      Bm[nl] = nullptr;
+      ++nl;
+    }
+    if (N[1] < N[0]) {
+      const uint32_t* t = L[0];
+      L[0] = L[1];
+      L[1] = t;
+      t = Bm[0];
+      Bm[0] = Bm[1];
+      Bm[1] = t;
+      const uint32_t tn = N[0];
+      N[0] = N[1];
+      N[1] = tn;
+    }
+    BoundsT<0> bd = MakeBounds<0>(s.cond, F, p);
+    uint32_t r0 = 0, r1 = 0;
+    Range(L[0], N[0], bd, r0, r1);
+    if (tid == 0) bytes += 4ULL * (r1 - r0) * 2ULL;
+    // the other list's window [a, e) over the pivot's value range
+    const uint32_t* W = L[1];
+    uint32_t WN = N[1];
+    bool staged = false;
+    uint32_t pad = 0;
+    if (!Bm[1] && r1 > r0) {
+      const uint32_t a = LowerBound(L[1], N[1], __ldg(L[0] + r0));
+      const uint32_t e = a + LowerBound(L[1] + a, N[1] - a, __ldg(L[0] + r1 - 1) + 1);
+      W = L[1] + a;
+      WN = e - a;
+      const uintptr_t lo = (uintptr_t)W, hi = (uintptr_t)(W + WN);
+      const uintptr_t alo = (lo + 15) & ~(uintptr_t)15, ahi = hi & ~(uintptr_t)15;
+      const uint32_t head = (uint32_t)((alo - lo) >> 2);  // elements before the aligned interior
+      pad = (4 - (head & 3)) & 3;
+      staged = WN >= 64 && pad + WN <= win_cap && WN <= kStageRatio * (r1 - r0) && ahi > alo;
+      if (staged) {
+        const uint32_t bytes_in = (uint32_t)(ahi - alo);
+        if (tid == 0) {
+          // shared memory the previous path read is overwritten by the async proxy
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes_in)
+                       : "memory");
+          const uint32_t dst = (uint32_t)__cvta_generic_to_shared(win + pad + head);
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+              "l"(alo), "r"(bytes_in), "r"(bar)
+              : "memory");
+        }
+        // ragged ends by plain loads
+        const uint32_t tail0 = (uint32_t)((ahi - lo) >> 2);
+        if (tid < (int)head) win[pad + tid] = __ldg(W + tid);
+        if (tid >= 4 && tid < 4 + (int)(WN - tail0)) win[pad + tail0 + (tid - 4)] = __ldg(W + tail0 + (tid - 4));
+        const bool done = MbarWait(bar, phase);
+        // one decision for the whole CTA (and the ragged ends made visible)
+        if (__syncthreads_or(!done)) {
+          // the copy did not complete: flag it, give it one more bounded
+          // wait (it writes this CTA's shared memory) and stop this CTA
+          if (tid == 0) atomicOr(err, ENGINE_ERR_TIMEOUT);
+          MbarWait(bar, phase);
+          return;
+        }
+        phase ^= 1;
+      }
+    }
+    const uint32_t* Ws = staged ? win + pad : W;
+    const uint32_t* Bo = Bm[1];
+    const uint32_t* P2 = nullptr;  // ranked-count partner set
+    uint32_t P2N = 0;
+    if (MODE == 1 && s.with_u >= 0) GetSet(F, s.with_u, p, P2, P2N);
+    const uint64_t out_off = MODE == 0 ? (p + b0 == 0 ? 0 : est_incl[p + b0 - 1]) - base : 0;
+    uint32_t cur = 0, written = 0;
+    for (uint32_t bi = r0; bi < r1; bi += CTA_THREADS) {
+      const uint32_t k = bi + tid;
+      bool ok = k < r1;
+      const uint32_t x = ok ? __ldg(L[0] + k) : 0;
+      if (ok && nl == 2) {
+        if (Bo) {
+          ok = BitTest(Bo, x);
+        } else if (staged) {
+          const uint32_t pos = cur + LowerBoundShared(Ws + cur, WN - cur, x);
+          cur = pos;
+          ok = pos < WN && Ws[pos] == x;
+        } else {
+          const uint32_t pos = cur + LowerBound(Ws + cur, WN - cur, x);
+          cur = pos;
+          ok = pos < WN && __ldg(Ws + pos) == x;
+        }
+      }
+      const unsigned mask = __ballot_sync(FULL, ok);
+      if (MODE == 1) {
+        if (ok) local += P2 ? RankCount(P2, P2N, x, s.with_op) : 1ULL;
+      } else {
+        if (lane == 0) wtot[wid] = __popc(mask);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < CTA_WARPS; ++w) {
+          const uint32_t c = wtot[w];
+          before += w < wid ? c : 0;
+          total += c;
+        }
+        if (MODE == 0 && ok) {
+          const uint64_t o = out_off + written + before + __popc(mask & ((1u << lane) - 1));
+          if (o < out_cap) out_data[o] = x;
+          else atomicOr(err, ENGINE_ERR_BOUNDS);
+        }
+        written += total;
+        __syncthreads();  // wtot is rewritten by the next chunk
+      }
+    }
+    if (tid == 0 && MODE != 1) {
+      out_ptr[p] = MODE == 0 ? (uint64_t)(out_data + out_off) : 0;
+      out_cnt[p] = written;
+      if (MODE == 0) bytes += 4ULL * written;
+    }
+    __syncthreads();  // the window is free for the next path
+  }
+  if (MODE == 1) {
+    local = WarpSum(local);
+    if (lane == 0 && local) atomicAdd(acc, local);
+  }
+  if (tid == 0 && bytes) atomicAdd(acc + 1, bytes);
 }
 
 // ---- intersection, flattened over 32 paths per warp ------------------------
@@ -1079,7 +1298,10 @@ class Executor {
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     CK(cudaGetLastError());
-    if (h[3]) Fail(SME_ERR_CUDA, "device bounds check failed (engine error flags " + std::to_string(h[3]) + ")");
+    if (h[3])
+      Fail(SME_ERR_CUDA, std::string(h[3] & ENGINE_ERR_BOUNDS ? "device bounds check failed" : "") +
+                             (h[3] & ENGINE_ERR_TIMEOUT ? " bulk-copy wait gave up" : "") + " (engine error flags " +
+                             std::to_string(h[3]) + ")");
     RunResult r;
     r.count = prog_.enumerate ? h[2] : h[0];
     r.emitted = h[2];
@@ -1177,16 +1399,30 @@ class Executor {
   }
   unsigned WarpGrid(uint64_t paths) const { return Grid(paths * 32, WARP_BLOCK); }
 
+  // Window of k_compute_cta in dynamic shared memory (64 KiB: two CTAs of
+  // 512 threads per SM), the attribute set once per device.
+  template <int MODE>
+  size_t CtaWindowBytes() {
+    constexpr size_t kBytes = 64 << 10;
+    static bool set[64] = {false};
+    const int d = ctx_.device;
+    if (d >= 0 && d < 64 && !set[d]) {
+      CK(cudaFuncSetAttribute(k_compute_cta<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBytes));
+      set[d] = true;
+    }
+    return kBytes;
+  }
+
   template <int MODE, int MINB, int NLM>
   void LaunchWarp(bool ne, const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est, uint32_t b0,
                   uint64_t* ptr, uint32_t* cnt, uint32_t* data, uint64_t cap, unsigned long long* acc,
                   uint32_t* err) {
     if (ne)
       k_compute<MODE, MINB, NLM, MAXV><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data,
-                                                                             cap, acc, err);
+                                                                             cap, acc, err, DHeavy{});
     else
       k_compute<MODE, MINB, NLM, 0><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap,
-                                                                          acc, err);
+                                                                          acc, err, DHeavy{});
   }
 
   template <int MODE, int MINB, int NLM>
@@ -1211,7 +1447,24 @@ class Executor {
     uint32_t* err = (uint32_t*)(ctrl_ + 3);
     Timed t = TimerStart();
     const int gran = gran_;
-    if (gran == 0 || gran == 3) {
+    const int nlists = ds.nconn + (ds.reuse >= 0 ? 1 : 0);
+    bool has_ne = false;
+    for (int i = 0; i < ds.cond.n; ++i) has_ne |= ds.cond.op[i] == 2;
+    if (gran == 4 && nlists == 2 && !has_ne) {
+      // warp per path; paths with a long clipped pivot go to a CTA each
+      const size_t mark = A_.Mark();
+      const uint32_t qcap = (uint32_t)std::min<uint64_t>(F.P, 1u << 16);
+      uint32_t* q = (uint32_t*)A_.Alloc(((size_t)qcap + 1) * 4);
+      CK(cudaMemsetAsync(q, 0, 4, st_));
+      k_compute<MODE, 8, 2, 0, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
+          F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, DHeavy{q, qcap, heavy_min_});
+      Launched();
+      const size_t win_bytes = CtaWindowBytes<MODE>();
+      k_compute_cta<MODE><<<(unsigned)sms_ * 2, CTA_THREADS, win_bytes, st_>>>(
+          F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, q, qcap, (uint32_t)(win_bytes / 4));
+      hot_ += 1;
+      A_.Release(mark);
+    } else if (gran == 0 || gran == 3 || gran == 4) {
       // warp per path, specialised on the number of intersected lists and
       // on the presence of `!=` conditions; fewer live values let more warps
       // reside, which is what counts: the searches are L2-latency bound.
@@ -1220,7 +1473,7 @@ class Executor {
       const int nl = ds.nconn + (ds.reuse >= 0 ? 1 : 0);
       bool ne = false;
       for (int i = 0; i < ds.cond.n; ++i) ne |= ds.cond.op[i] == 2;
-      const bool dense = gran == 0;
+      const bool dense = gran != 3;
       if (nl <= 2)
         dense ? LaunchWarp<MODE, 8, 2>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err)
               : LaunchWarp<MODE, 6, 2>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
@@ -1230,7 +1483,8 @@ class Executor {
       else
         LaunchWarp<MODE, 6, MAXV>(ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
     } else if (gran == 1) {
-      k_compute<MODE><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+      k_compute<MODE><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(F, ds, G, est, b0, ptr, cnt, data, cap, acc, err,
+                                                             DHeavy{});
     } else {
       // flattened, specialised the same way
       const int nl = ds.nconn + (ds.reuse >= 0 ? 1 : 0);
@@ -1249,6 +1503,7 @@ class Executor {
 
  public:
   int gran_ = 0;
+  uint32_t heavy_min_ = 2048;  // granularity 4: shortest pivot that gets a CTA
   bool use_bitmaps_ = true;
 
  private:
@@ -1528,6 +1783,7 @@ RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& c
   Executor ex(prog, g, ctx, d_out, cap);
   ex.gran_ = tuning & 0xff;
   ex.use_bitmaps_ = !(tuning & 0x100);
+  if (const char* e = std::getenv("SME_HEAVY_PIVOT")) ex.heavy_min_ = (uint32_t)std::max(32L, std::atol(e));
   return ex.Run(t);
 }
 

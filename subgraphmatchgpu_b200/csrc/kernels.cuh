@@ -16,7 +16,18 @@ namespace dev {
 constexpr int MAXV = 6;  // kMaxQueryVerticesNum, src/Meta.h:30
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int WARP_BLOCK = 256;  // threads per block of warp-per-path kernels
-constexpr uint32_t ENGINE_ERR_BOUNDS = 1u;  // a write would leave its buffer
+constexpr uint32_t ENGINE_ERR_BOUNDS = 1u;   // a write would leave its buffer
+constexpr uint32_t ENGINE_ERR_TIMEOUT = 2u;  // a bounded wait on a bulk copy gave up
+
+// Paths whose clipped pivot is long are handed from the warp-per-path
+// intersection to a CTA per path: `q[0]` counts the deferred paths, their
+// indices follow (at most `cap`); a path that finds the queue full stays
+// with its warp.  q == nullptr: nothing is deferred.
+struct DHeavy {
+  uint32_t* q;
+  uint32_t cap;
+  uint32_t min_len;
+};
 
 struct DSet {
   const uint64_t* ptr;  // absolute device address of the first element

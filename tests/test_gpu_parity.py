@@ -49,6 +49,29 @@ def test_intersection_granularities(graphs, golden, gran):
         assert np.array_equal(got, O.enumerate_sorted(rp, cl, q))
 
 
+@pytest.mark.parametrize("threshold", ["32", "256"])
+def test_long_pivot_paths_on_a_cta_each(graphs, golden, threshold, monkeypatch):
+    # granularity 4: two-list steps hand paths whose clipped pivot holds at
+    # least SME_HEAVY_PIVOT elements to a CTA each (the other list staged in
+    # shared memory by a bulk copy when it is not a hub); a low threshold
+    # sends many paths there on the small graphs
+    monkeypatch.setenv("SME_HEAVY_PIVOT", threshold)
+    for name in ("rmat_s12_ef8", "ba_n600_m4", "rmat_s10_ef8", "k20"):
+        for q, want in golden[name]["counts"].items():
+            if want > GPU_LIMIT:
+                continue
+            for algo in ALGOS:
+                got = graphs[name].count(int(q), algo, warp_granularity=4)
+                assert got == want, (name, q, algo, threshold, got, want)
+                got = graphs[name].count(int(q), algo, warp_granularity=4, list_only=1)
+                assert got == want, (name, q, algo, threshold, "list_only", got, want)
+    for name in ("er_n64_d12", "ba_n600_m4"):
+        rp, cl = O.read_bin(golden_graph_path(name))
+        for q in (0, 3, 4, 2):
+            got = O.sort_rows(graphs[name].enumerate(q, sme.GPU_LIGHT, warp_granularity=4))
+            assert np.array_equal(got, O.enumerate_sorted(rp, cl, q)), (name, q)
+
+
 @pytest.mark.parametrize("level", [0, 1, 2, 3])
 def test_light_compress_levels(graphs, golden, level):
     for name in ("rmat_s10_ef8", "ba_n600_m4", "k12"):
