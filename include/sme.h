@@ -131,6 +131,9 @@ typedef struct sme_stats {
    * [4] compute_path_count, [5] count, [6] organize_batch (estimates, scans),
    * [7] external subgraph load. */
   double phase_ms[8];
+  uint64_t reuse_hits;        /* reuse plan: paths whose mapped reuse found the
+                                 sibling's cached intersection (the rest
+                                 intersected the adjacency lists)            */
 } sme_stats;
 
 /* ---- options ------------------------------------------------------------- */

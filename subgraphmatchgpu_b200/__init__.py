@@ -61,6 +61,7 @@ class Stats(C.Structure):
         ("batches", C.c_uint64), ("algorithmic_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64),
         ("d2h_bytes", C.c_uint64), ("peak_device_bytes", C.c_uint64), ("paths_processed", C.c_uint64),
         ("device_ms", C.c_double), ("hot_launches", C.c_uint64), ("phase_ms", C.c_double * 8),
+        ("reuse_hits", C.c_uint64),
     ]
 
     PHASES = ("compute", "materialize", "filter_compute", "compute_count", "compute_path_count", "count",

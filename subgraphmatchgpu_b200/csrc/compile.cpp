@@ -130,25 +130,50 @@ Program CompileReuse(const Query& q, bool autogen, bool enumerate) {
     Step c;
     c.u = (uint8_t)u;
     c.full_conn = U8(oc[u]);
-    // Reuse one ancestor cache (identity mapping on the prefix); any other
-    // reuse meta is intersected from its adjacency lists instead.
+    // Reuse one ancestor cache (identity mapping on the prefix).  A meta
+    // whose mapping keeps level 0 and moves level 1 to an earlier vertex x
+    // (the intersection N(M[0]) ∩ N(M[x]) cached at level 2 by the sibling
+    // path (M[0], M[x])) is located at run time (FindCacheOffsets,
+    // src/gpu/impl/common/CheckConstraintsReuseCommon.cuh:14-112); its
+    // adjacency lists stay in `conn` for the paths whose sibling is not in
+    // the current batch.  Any other meta is intersected from its lists.
     std::vector<uint8_t> conn = U8(vp.separate);
+    std::vector<uint8_t> others = conn;  // lists not covered by the mapped meta
     int src = -1;
+    const ReuseConnMeta* sib = nullptr;
     for (auto& r : vp.reuse) {
       bool ancestor = r.source_vertex < (uintV)u && r.mapping.size() == (size_t)n &&
                       r.mapping[r.source_vertex] == (uintV)u;
       for (uintV x = 0; ancestor && x < r.source_vertex; ++x)
         if (r.mapping[x] != x) ancestor = false;
+      const bool sibling = !ancestor && !sib && r.source_vertex == 2 && r.mapping.size() == (size_t)n &&
+                           r.source_conn == ConnType{0, 1} && r.mapping[0] == 0 && r.mapping[1] >= 2 &&
+                           r.mapping[1] < (uintV)u && rp.cache_required[2];
       if (ancestor && src < 0 && rp.cache_required[r.source_vertex]) {
         src = (int)r.source_vertex;
       } else {
         for (uintV x : r.conn) conn.push_back((uint8_t)x);
+        if (sibling) sib = &r;
+        else
+          for (uintV x : r.conn) others.push_back((uint8_t)x);
       }
     }
     std::sort(conn.begin(), conn.end());
     conn.erase(std::unique(conn.begin(), conn.end()), conn.end());
     c.conn = conn;
     c.reuse_src = (int8_t)src;
+    if (sib) {
+      // the cached set replaces exactly the meta's lists, none of which any
+      // other source of this step also asks for
+      bool clash = false;
+      for (uintV x : sib->conn) clash = clash || std::count(others.begin(), others.end(), (uint8_t)x) > 0;
+      if (!clash) {
+        c.map_src = 2;
+        c.map_x = (uint8_t)sib->mapping[1];
+        for (size_t i = 0; i < conn.size(); ++i)
+          if (std::count(sib->conn.begin(), sib->conn.end(), (uintV)conn[i])) c.map_mask |= (uint8_t)(1u << i);
+      }
+    }
     if (rp.cache_required[u] && !last) {
       // intersect-only result kept as the cache; conditions at materialise
       c.kind = S_COMPUTE;
@@ -446,6 +471,39 @@ Program CompileLight(const Query& q, int compress_level, bool enumerate, bool se
 }
 }  // namespace
 
+// A mapped reuse step finds its sibling's cached set by the rank of the
+// sibling's level-1 vertex in N(M[0]).  That holds only while the level-1
+// candidates of a root are all of N(M[0]) in order (COMPUTE(1) over {0}
+// with no condition, MATERIALIZE(1) with none) and the level-2 cache is the
+// plain intersection N(M[0]) ∩ N(M[1]); otherwise the step keeps its lists.
+static void RequireSiblingLayout(Program& p) {
+  auto find = [&](StepKind k, uint8_t u) -> const Step* {
+    for (const Step& s : p.steps)
+      if (s.kind == k && s.u == u) return &s;
+    return nullptr;
+  };
+  const Step* c1 = find(S_COMPUTE, 1);
+  const Step* m1 = find(S_MATERIALIZE, 1);
+  const Step* c2 = find(S_COMPUTE, 2);
+  // level 1 may clip N(M[0]) by one order condition against M[0] (the clip
+  // cancels out of the rank difference once M[x] passes it)
+  const bool clip = c1 && c1->cond.size() == 1 && c1->cond[0].operand == 0 && c1->cond[0].op != OP_NONE &&
+                    c1->cond[0].op != 2;
+  const bool ok = c1 && m1 && c2 && (c1->cond.empty() || clip) && m1->cond.empty() && c1->reuse_src < 0 &&
+                  c1->conn == std::vector<uint8_t>{0} && c2->cond.empty() && c2->reuse_src < 0 &&
+                  c2->conn == std::vector<uint8_t>{0, 1};
+  for (Step& s : p.steps) {
+    if (s.map_src < 0) continue;
+    if (!ok) {
+      s.map_src = -1;
+      s.map_x = 0;
+      s.map_mask = 0;
+    } else {
+      s.map_op = clip ? c1->cond[0].op : OP_NONE;
+    }
+  }
+}
+
 Program Compile(const sme_opts& o, bool enumerate, bool loop_free) {
   Query q(o.query_type, o.enable_ordering != 0);
   Program p;
@@ -470,6 +528,7 @@ Program Compile(const sme_opts& o, bool enumerate, bool loop_free) {
   p.algo = o.algo;
   p.enumerate = enumerate;
   PruneImpliedExclusions(p, loop_free);
+  RequireSiblingLayout(p);
   for (auto& s : p.steps) {
     std::ostringstream os;
     os << KindName(s.kind) << "(" << (int)s.u << ")";
@@ -516,6 +575,9 @@ std::string Program::Describe() const {
       os << ")";
     }
     if (s.reuse_src >= 0) os << " reuse=" << (int)s.reuse_src;
+    if (s.map_src >= 0)
+      os << " sibling=(" << (int)s.map_src << ",x=" << (int)s.map_x
+         << (s.map_op == 0 ? ",<0" : s.map_op == 1 ? ",>0" : "") << ")";
     if (!s.cond.empty()) {
       os << " cond=(";
       for (size_t j = 0; j < s.cond.size(); ++j)

@@ -200,6 +200,35 @@ __global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __res
   }
 }
 
+// ---- mapped reuse: the sibling path's cached intersection ----------------
+// In the reuse plan the level-1 paths of a root M[0] are its neighbours N(M[0])
+// in order (one contiguous run per root; the compiler checks level 1 has no
+// condition), and the level-2 store holds, per level-1 path (M[0], y) of the
+// current batch, the intersection N(M[0]) ∩ N(y).  A path whose ancestor is
+// (M[0], M[1]) at store index s finds the sibling (M[0], M[x]) at index
+// s + rank(M[x]) - rank(M[1]), ranks taken in N(M[0]) (FastLocateCache over
+// the prefix tree, src/gpu/impl/common/CheckConstraintsReuseCommon.cuh:114-289,
+// reduced to two binary searches by that layout).  `sib` stays null when the
+// sibling is not in the store (another batch), and the step intersects the
+// lists instead.
+__device__ __forceinline__ void SiblingSet(const DFront& F, const DStep& s, const DGraph& G, uint32_t p,
+                                           const uint32_t*& sib, uint32_t& sibn) {
+  sib = nullptr;
+  sibn = 0;
+  if (s.msrc < 0) return;
+  const uint32_t m0 = F.inst[0][p], m1 = F.inst[1][p], mx = F.inst[s.mx][p];
+  if ((s.mop == 0 && !(mx < m0)) || (s.mop == 1 && !(mx > m0))) return;  // not a level-1 candidate
+  const uintE b = G.rp[m0];
+  const uint32_t d0 = (uint32_t)(G.rp[m0 + 1] - b);
+  const uint32_t* n0 = G.cols + b;
+  const uint32_t ia = LowerBound(n0, d0, m1), ib = LowerBound(n0, d0, mx);
+  if (ib >= d0 || __ldg(n0 + ib) != mx) return;
+  const int64_t s2 = (int64_t)SetIndex(F, s.msrc, p) + (int64_t)ib - (int64_t)ia;
+  if (s2 < 0 || s2 >= (int64_t)F.nset[s.msrc]) return;
+  sib = reinterpret_cast<const uint32_t*>(F.set[s.msrc].ptr[s2]);
+  sibn = F.set[s.msrc].cnt[s2];
+}
+
 // ---- intersection (COMPUTE / COMPUTE_COUNT / COMPUTE_PATH_COUNT) ---------
 // One warp per path.  The pivot is the smallest list (ThreadChoosePivotLevel,
 // CheckConstraintsCommon.cuh:10-29); < and > conditions clip the pivot to a
@@ -215,8 +244,10 @@ __global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __res
 // without `!=` conditions (no exclusion array).  The launcher guarantees
 // both bounds.
 // DEFER (two lists, no `!=`): a path whose clipped pivot holds at least
-// hv.min_len elements is queued for k_compute_cta instead.
-template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV, bool DEFER = false>
+// hv.min_len elements is queued for k_compute_cta instead.  MAPPED (reuse
+// plan, s.msrc >= 0): the set cached by the sibling path replaces the lists
+// of s.mmask when the sibling is in the current batch (see SiblingSet).
+template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV, bool DEFER = false, bool MAPPED = false>
 __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
     uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err,
@@ -227,7 +258,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   const unsigned lt = (1u << lane) - 1;
-  unsigned long long local = 0, bytes = 0;
+  unsigned long long local = 0, bytes = 0, hits = 0;
   const uint64_t base = b0 == 0 ? 0 : est_incl[b0 - 1];
 
   for (uint32_t p = gw; p < F.P; p += nw) {
@@ -235,16 +266,47 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     const uint32_t* B[NLM];  // hub bitmap of the list (null: binary search)
     uint32_t N[NLM];
     int nl = 0;
+    const uint32_t* sib = nullptr;
+    uint32_t sibn = 0;
+    if constexpr (MAPPED) SiblingSet(F, s, G, p, sib, sibn);
+    if (MAPPED && sib) {
+      // the lists outside the mask, then the sibling's cached set
 #pragma unroll
-    for (int i = 0; i < NLM; ++i) {
-      B[i] = nullptr;
-      if (i < s.nconn) {
-        uint32_t v = F.inst[s.conn[i]][p];
-        uintE b = rp[v], e = rp[v + 1];
-        L[i] = cols + b;
-        N[i] = (uint32_t)(e - b);
-        B[i] = HubBitmap(G, v);
-        nl = i + 1;
+      for (int i = 0; i < NLM; ++i) {
+        if (i < s.nconn && !((s.mmask >> i) & 1)) {
+          const uint32_t v = F.inst[s.conn[i]][p];
+          const uintE b = rp[v], e = rp[v + 1];
+#pragma unroll
+          for (int t = 0; t < NLM; ++t)
+            if (t == nl) {
+              L[t] = cols + b;
+              N[t] = (uint32_t)(e - b);
+              B[t] = HubBitmap(G, v);
+            }
+          ++nl;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < NLM; ++t)
+        if (t == nl) {
+          L[t] = sib;
+          N[t] = sibn;
+          B[t] = nullptr;
+        }
+      ++nl;
+      if (lane == 0) ++hits;
+    } else {
+#pragma unroll
+      for (int i = 0; i < NLM; ++i) {
+        B[i] = nullptr;
+        if (i < s.nconn) {
+          uint32_t v = F.inst[s.conn[i]][p];
+          uintE b = rp[v], e = rp[v + 1];
+          L[i] = cols + b;
+          N[i] = (uint32_t)(e - b);
+          B[i] = HubBitmap(G, v);
+          nl = i + 1;
+        }
       }
     }
     if (s.reuse >= 0) {
@@ -362,6 +424,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     if (lane == 0 && local) atomicAdd(acc, local);
   }
   if (lane == 0 && bytes) atomicAdd(acc + 1, bytes);
+  if (MAPPED && lane == 0 && hits) atomicAdd(acc + 5, hits);
 }
 
 // ---- intersection, one CTA per long-pivot path ----------------------------
@@ -1236,6 +1299,10 @@ DStep ToDStep(const Step& s) {
   d.cond = ToDCond(s.cond);
   d.with_u = s.with_u;
   d.with_op = s.with_op;
+  d.msrc = s.map_src;
+  d.mx = s.map_x;
+  d.mmask = s.map_mask;
+  d.mop = s.map_op;
   return d;
 }
 
@@ -1306,6 +1373,7 @@ class Executor {
     r.count = prog_.enumerate ? h[2] : h[0];
     r.emitted = h[2];
     r.stats.algorithmic_bytes = h[1];
+    r.stats.reuse_hits = h[5];
     r.stats.kernel_launches = launches_;
     r.stats.batches = batches_;
     r.stats.peak_device_bytes = A_.peak;
@@ -1340,7 +1408,7 @@ class Executor {
   uint32_t* out_;
   uint64_t cap_;
   int sms_ = 148;
-  unsigned long long* ctrl_ = nullptr;  // [0] count [1] bytes [2] emitted [3] error flags
+  unsigned long long* ctrl_ = nullptr;  // [0] count [1] bytes [2] emitted [3] error flags [5] reuse hits
   uint64_t launches_ = 0, batches_ = 0, paths_ = 0, hot_ = 0, root_h2d_ = 0;
   const uint32_t* ext_cols_ = nullptr;
   uint64_t ext_bytes_ = 0;
@@ -1450,7 +1518,15 @@ class Executor {
     const int nlists = ds.nconn + (ds.reuse >= 0 ? 1 : 0);
     bool has_ne = false;
     for (int i = 0; i < ds.cond.n; ++i) has_ne |= ds.cond.op[i] == 2;
-    if (gran == 4 && nlists == 2 && !has_ne) {
+    if (ds.msrc >= 0) {
+      // mapped reuse: the warp kernel that looks up the sibling's set
+      if (has_ne)
+        k_compute<MODE, 4, MAXV, MAXV, false, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
+            F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, DHeavy{});
+      else
+        k_compute<MODE, 4, MAXV, 0, false, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
+            F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, DHeavy{});
+    } else if (gran == 4 && nlists == 2 && !has_ne) {
       // warp per path; paths with a long clipped pivot go to a CTA each
       const size_t mark = A_.Mark();
       const uint32_t qcap = (uint32_t)std::min<uint64_t>(F.P, 1u << 16);
@@ -1703,6 +1779,7 @@ class Executor {
             Compute<2>(Fb, ds, gv, est, b.b0, ptr, cnt, nullptr, 0);
           DFront Fn = Fb;
           Fn.set[s.u] = DSet{ptr, cnt};
+          Fn.nset[s.u] = Pb;
           Fn.cidx[s.u] = nullptr;
           Fn.ident_off[s.u] = 0;
           Level(k + 1, Fn);
@@ -1720,6 +1797,7 @@ class Executor {
           Launched();
           DFront Fn = Fb;
           Fn.set[s.u] = DSet{ptr, cnt};
+          Fn.nset[s.u] = Pb;
           Fn.cidx[s.u] = nullptr;
           Fn.ident_off[s.u] = 0;
           Level(k + 1, Fn);
@@ -1756,6 +1834,7 @@ class Executor {
           for (int v = 0; v < MAXV; ++v) Fn.inst[v] = o.inst[v];
           for (uint8_t w : s.sets_after) {
             Fn.set[w] = Fb.set[w];
+            Fn.nset[w] = Fb.nset[w];
             Fn.cidx[w] = o.cidx[w];
           }
           Level(k + 1, Fn);

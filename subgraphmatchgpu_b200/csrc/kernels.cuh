@@ -40,6 +40,7 @@ struct DFront {
   const uint32_t* cidx[MAXV];     // set index per path (null: identity)
   uint32_t ident_off[MAXV];       // identity index offset (after slicing)
   DSet set[MAXV];                 // candidate-set stores
+  uint32_t nset[MAXV];            // sets in each store
 };
 
 struct DCond {
@@ -56,6 +57,14 @@ struct DStep {
   DCond cond;
   int8_t with_u;  // COMPUTE_COUNT rank partner (-1 none)
   uint8_t with_op;
+  // reuse plan, a mapped reuse meta: the sibling path (M[0], M[mx]) of the
+  // current path's level-1 ancestor holds, in the cached store of vertex
+  // msrc, the intersection that replaces the lists conn[i] with bit i of
+  // mmask set (msrc < 0: none)
+  int8_t msrc;
+  uint8_t mx;
+  uint8_t mmask;
+  uint8_t mop;  // level 1's order against M[0] the sibling's vertex obeys (0 <, 1 >, else none)
 };
 
 struct DMatOut {

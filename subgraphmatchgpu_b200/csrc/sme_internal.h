@@ -175,6 +175,10 @@ struct Step {
   std::vector<uint8_t> conn;      // materialised vertices: adjacency lists
   int8_t reuse_src = -1;          // vertex whose cached set is intersected
   std::vector<uint8_t> full_conn; // fallback when no cache (reuse plan)
+  int8_t map_src = -1;            // reuse plan: mapped meta's cached level
+  uint8_t map_x = 0;              //   vertex in the sibling's level-1 place
+  uint8_t map_mask = 0;           //   conn entries the cached set replaces
+  uint8_t map_op = OP_NONE;       //   level 1's order condition against M[0]
   std::vector<StepCond> cond;     // conditions vs materialised vertices
   bool keep_set = false;          // MATERIALIZE keeps u's set as a cache
   int8_t with_u = -1;             // COMPUTE_COUNT rank partner

@@ -128,6 +128,27 @@ def test_root_ranges_sum_to_total(graphs, golden):
         assert parts == golden["rmat_s12_ef8"]["counts"][str(q)]
 
 
+@pytest.mark.parametrize("q", [5, 9, 10, 13])
+def test_reuse_plan_locates_sibling_caches(graphs, golden, q):
+    # the hard-coded reuse plans of Q5, Q9, Q10 and Q13 reuse, at a later
+    # level, the level-2 intersection N(M0) ∩ N(M[x]) a sibling path cached;
+    # the engine finds it by rank in N(M0) and falls back to the adjacency
+    # lists when the sibling is in another batch (a small budget forces many)
+    name = "rmat_s10_ef8"
+    want = golden[name]["counts"][str(q)]
+    g = graphs[name]
+    assert "sibling=(2" in sme.plan_describe(q, 6).split("algo=5")[1].split("program")[0]
+    assert g.count(q, sme.GPU_GPSM_REUSE) == want
+    hits = sme.last_stats().reuse_hits
+    assert hits > 0
+    assert g.count(q, sme.GPU_GPSM_REUSE, mem_limit_bytes=4 << 20) == want
+    assert sme.last_stats().batches > 1
+    for name2 in ("ba_n600_m4", "er_n64_d12", "k12"):
+        w = golden[name2]["counts"].get(str(q))
+        if w is not None and w <= GPU_LIMIT:
+            assert graphs[name2].count(q, sme.GPU_GPSM_REUSE) == w, name2
+
+
 def test_small_memory_budget_forces_many_batches(graphs, golden):
     g = graphs["rmat_s12_ef8"]
     for algo in ALGOS:
