@@ -308,6 +308,35 @@ def reference_graph(args, tmpdir):
     return None, *O.preprocess_csr(rp, cl)
 
 
+def calibrate_c1(threads, tmp):
+    """The reference's unmodified CPU program (patternmatchcpu -a 0 -q 0) on
+    the triangle configuration (R-MAT s14 ef8, the reference's own
+    elapsed_time=, src/cpu/PatternMatchCPU.cpp:55-62 and CPUWCOJ.h:58-60),
+    beside the root-task driver over all roots of the same BIN: the driver
+    runs the same DFS, so their times should agree."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "patternmatchcpu")
+    if not (os.path.exists(binary) and os.path.exists(REF_TASK) and os.path.exists(REF_PREPROCESS)):
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py as O
+    u, v = rmat_edges(14, 8, seed=14)
+    txt = os.path.join(tmp, "c1.txt")
+    O.write_edge_text(u, v, txt)
+    subprocess.run([REF_PREPROCESS, "-f", txt, "-d", "0"], capture_output=True, text=True, check=True)
+    out = subprocess.run([binary, "-f", txt + ".bin", "-d", "0", "-a", "0", "-q", "0", "-t", str(threads)],
+                         capture_output=True, text=True, check=True).stdout
+    line = next(ln for ln in out.splitlines() if ln.startswith("total_match_count="))
+    kv = dict(x.strip().split("=", 1) for x in line.split(","))
+    c, ms = int(kv["total_match_count"]), float(kv["elapsed_time"].rstrip("ms"))
+    drv = subprocess.run([REF_TASK, "-f", txt + ".bin", "-q", "0", "-t", str(threads), "S:1:0"],
+                         capture_output=True, text=True, check=True).stdout
+    dk = dict(x.strip().split("=", 1) for x in next(ln for ln in drv.splitlines() if ln.startswith("task=")).split(","))
+    return {"workload": "R-MAT s14 ef8 seed 14, triangle, whole graph", "threads": threads,
+            "patternmatchcpu": {"instances": c, "elapsed_ms": ms, "value": c / (ms / 1e3) if ms > 0 else 0.0},
+            "ref_wcoj_task": {"instances": int(dk["total_match_count"]),
+                              "elapsed_ms": float(dk["elapsed_time"].rstrip("ms"))}}
+
+
 def run_reference(args, rank, world):
     """CPU reference arm: the reference's own CPU_WCOJ on the host cores, the
     same steps as the engine's arm (rank 0 only; other ranks exit)."""
@@ -325,6 +354,10 @@ def run_reference(args, rank, world):
         else:
             res = port_tasks(rp, cl, steps, threads)
             kind, what = "port", "the oracle's C restatement of CPU_WCOJ (the reference's tools were not built)"
+        try:
+            c1 = calibrate_c1(threads, tmp)
+        except Exception as ex:  # reported in the line, never dropped silently
+            c1 = {"error": f"{type(ex).__name__}: {ex}"}
     timed = list(zip(steps, res))[args.warmup:]
     inst = sum(c for _, (c, _) in timed)
     ms = sum(t for _, (_, t) in timed)
@@ -344,7 +377,7 @@ def run_reference(args, rank, world):
             "config": config_of(args, n, m, csr_digest(rp, cl)), "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "per_query": per_query_summary(per_q),
-            "step_counts": [int(c) for _, (c, _) in timed]}
+            "step_counts": [int(c) for _, (c, _) in timed], "c1_calibration": c1}
     print(json.dumps(line), flush=True)
 
 

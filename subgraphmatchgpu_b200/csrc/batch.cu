@@ -371,8 +371,11 @@ __global__ void k_noalloc_inspect(const uint64_t* __restrict__ rp, const uint32_
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    m = max(m, __shfl_down_sync(FULL, m, o));
-    bad = bad || __shfl_down_sync(FULL, (int)bad, o);
+    // every lane takes part in both shuffles (no short-circuit around one)
+    const unsigned int om = __shfl_down_sync(FULL, m, o);
+    const int ob = __shfl_down_sync(FULL, (int)bad, o);
+    m = max(m, om);
+    bad = bad || ob != 0;
   }
   if ((threadIdx.x & 31) == 0) {
     if (m) atomicMax(hdr + 4, m);

@@ -218,9 +218,9 @@ __device__ __forceinline__ void SiblingSet(const DFront& F, const DStep& s, cons
   if (s.msrc < 0) return;
   const uint32_t m0 = F.inst[0][p], m1 = F.inst[1][p], mx = F.inst[s.mx][p];
   if ((s.mop == 0 && !(mx < m0)) || (s.mop == 1 && !(mx > m0))) return;  // not a level-1 candidate
-  const uintE b = G.rp[m0];
-  const uint32_t d0 = (uint32_t)(G.rp[m0 + 1] - b);
-  const uint32_t* n0 = G.cols + b;
+  const uint32_t* n0;
+  uint32_t d0;
+  AdjList(G, m0, n0, d0);
   const uint32_t ia = LowerBound(n0, d0, m1), ib = LowerBound(n0, d0, mx);
   if (ib >= d0 || __ldg(n0 + ib) != mx) return;
   const int64_t s2 = (int64_t)SetIndex(F, s.msrc, p) + (int64_t)ib - (int64_t)ia;
@@ -252,8 +252,6 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
     uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err,
     DHeavy hv) {
-  const uintE* __restrict__ rp = G.rp;
-  const uint32_t* __restrict__ cols = G.cols;
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
@@ -275,12 +273,14 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
       for (int i = 0; i < NLM; ++i) {
         if (i < s.nconn && !((s.mmask >> i) & 1)) {
           const uint32_t v = F.inst[s.conn[i]][p];
-          const uintE b = rp[v], e = rp[v + 1];
+          const uint32_t* lp;
+          uint32_t ln;
+          AdjList(G, v, lp, ln);
 #pragma unroll
           for (int t = 0; t < NLM; ++t)
             if (t == nl) {
-              L[t] = cols + b;
-              N[t] = (uint32_t)(e - b);
+              L[t] = lp;
+              N[t] = ln;
               B[t] = HubBitmap(G, v);
             }
           ++nl;
@@ -301,9 +301,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
         B[i] = nullptr;
         if (i < s.nconn) {
           uint32_t v = F.inst[s.conn[i]][p];
-          uintE b = rp[v], e = rp[v + 1];
-          L[i] = cols + b;
-          N[i] = (uint32_t)(e - b);
+          AdjList(G, v, L[i], N[i]);
           B[i] = HubBitmap(G, v);
           nl = i + 1;
         }
@@ -482,8 +480,6 @@ __global__ void __launch_bounds__(CTA_THREADS, 2) k_compute_cta(
   extern __shared__ __align__(128) uint32_t win[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t wtot[CTA_WARPS];
-  const uintE* __restrict__ rp = G.rp;
-  const uint32_t* __restrict__ cols = G.cols;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&mbar);
   if (tid == 0) {
@@ -504,9 +500,7 @@ __global__ void __launch_bounds__(CTA_THREADS, 2) k_compute_cta(
     int nl = 0;
     for (int k = 0; k < 2 && k < s.nconn; ++k) {
       const uint32_t v = F.inst[s.conn[k]][p];
-      const uintE b = rp[v], e = rp[v + 1];
-      L[k] = cols + b;
-      N[k] = (uint32_t)(e - b);
+      AdjList(G, v, L[k], N[k]);
       Bm[k] = HubBitmap(G, v);
       nl = k + 1;
     }
@@ -662,8 +656,6 @@ template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV>
 __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute_flat(
     DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
     uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err) {
-  const uintE* __restrict__ rp = G.rp;
-  const uint32_t* __restrict__ cols = G.cols;
   __shared__ FlatPath<NLM, NEX> sp[FLAT_WARPS][32];
   __shared__ uint32_t soff[FLAT_WARPS][33];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
@@ -686,9 +678,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute_flat(
         B[i] = nullptr;
         if (i < s.nconn) {
           uint32_t v = F.inst[s.conn[i]][p];
-          uintE b = rp[v], e = rp[v + 1];
-          L[i] = cols + b;
-          N[i] = (uint32_t)(e - b);
+          AdjList(G, v, L[i], N[i]);
           B[i] = HubBitmap(G, v);
           nl = i + 1;
         }
@@ -1036,49 +1026,57 @@ __global__ void k_count_direct(DFront F, uint8_t nu, uint8_t u0, uint8_t u1, uin
 // ---- external mode: per-batch subgraph ------------------------------------
 // Marks the adjacency lists a batch's intersections read
 // (InspectRequiredAdjLists, src/gpu/impl/common/ext/EXTGraphGPUCommon.cuh:157-184).
-__global__ void k_ext_mark(DFront F, DStep s, uint8_t* flag) {
+// External mode keeps the adjacency lists a batch reads in a device list
+// cache: coff[v] is the first element of v's list in the cache, kAbsent when
+// it is not there.  A batch claims the lists it needs that are missing
+// (IncInspectRequiredAdjLists, src/gpu/impl/common/ext/EXTIncGraphGPUCommon.cuh:20-75:
+// lists already in device memory are not loaded again), places them after
+// the cache's last list and gathers them from pinned, mapped host memory;
+// lists stay for later batches and steps until the cache is full, when it
+// starts over.  Only the lists of a batch cross the host link, and no work
+// scales with the vertex count except a start-over.
+constexpr uint64_t kAbsent = ~0ULL, kPending = ~0ULL - 1;
+
+__global__ void k_ext_claim(DFront F, DStep s, const uintE* __restrict__ rp, uint64_t* coff, uint32_t* newids,
+                            unsigned int* nnew) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.P; p += gridDim.x * blockDim.x)
-    for (int i = 0; i < s.nconn; ++i) flag[F.inst[s.conn[i]][p]] = 1;
+    for (int i = 0; i < s.nconn; ++i) {
+      const uint32_t v = F.inst[s.conn[i]][p];
+      if (rp[v + 1] == rp[v] || coff[v] != kAbsent) continue;
+      if (atomicCAS(reinterpret_cast<unsigned long long*>(coff + v), kAbsent, kPending) == kAbsent)
+        newids[atomicAdd(nnew, 1u)] = v;
+    }
 }
 
-// Degree of each required vertex (0 elsewhere) and the required flag, for the
-// subgraph's global-id row pointers (BuildSubgraphRowPtrs, EXTGraphGPUCommon.cuh:26-55).
-__global__ void k_ext_deg(const uint8_t* __restrict__ flag, const uintE* __restrict__ rp, uint32_t n,
-                          uint64_t* deg, uint64_t* fl) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    bool f = flag[v] != 0;
-    deg[v] = f ? rp[v + 1] - rp[v] : 0;
-    fl[v] = f ? 1 : 0;
-  }
+__global__ void k_ext_newdeg(const uint32_t* __restrict__ ids, uint32_t n, const uintE* __restrict__ rp,
+                             uint64_t* deg) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    deg[k] = rp[ids[k] + 1] - rp[ids[k]];
 }
 
-__global__ void k_ext_rowptr(const uint64_t* __restrict__ deg_incl, uint32_t n, uintE* sub_rp) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x)
-    sub_rp[v] = v == 0 ? 0 : deg_incl[v - 1];
+__global__ void k_ext_place(const uint32_t* __restrict__ ids, uint32_t n, const uint64_t* __restrict__ deg_incl,
+                            uint64_t used, uint64_t* coff) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    coff[ids[k]] = used + (k == 0 ? 0 : deg_incl[k - 1]);
 }
 
-__global__ void k_ext_ids(const uint8_t* __restrict__ flag, const uint64_t* __restrict__ fl_incl, uint32_t n,
-                          uint32_t* ids) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-    if (flag[v]) ids[fl_incl[v] - 1] = v;
-}
-
-// Copies the required lists from pinned, mapped host memory into the device
-// subgraph (one warp per list, coalesced reads over the host link); replaces
+// Copies the newly placed lists from pinned, mapped host memory into the
+// cache (one warp per list, coalesced reads over the host link); replaces
 // the host-thread gather + synchronous H2D of LoadSubgraph
 // (src/gpu/impl/common/ext/LoadSubgraph.h:10-42, EXTGraphGPUCommon.cuh:60-149).
 __global__ void __launch_bounds__(WARP_BLOCK) k_ext_gather(const uint32_t* __restrict__ ids, uint32_t nid,
                                                            const uintE* __restrict__ rp,
                                                            const uint32_t* __restrict__ host_cols,
-                                                           const uintE* __restrict__ sub_rp,
-                                                           uint32_t* __restrict__ sub_cols) {
+                                                           const uint64_t* __restrict__ coff,
+                                                           uint32_t* __restrict__ cache) {
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t i = gw; i < nid; i += nw) {
-    uint32_t v = ids[i];
-    uintE b = rp[v], e = rp[v + 1], o = sub_rp[v];
-    for (uintE j = b + lane; j < e; j += 32) sub_cols[o + (j - b)] = host_cols[j];
+    const uint32_t v = ids[i];
+    const uintE b = rp[v], e = rp[v + 1];
+    const uint64_t o = coff[v];
+    for (uintE j = b + lane; j < e; j += 32) cache[o + (j - b)] = host_cols[j];
   }
 }
 
@@ -1326,6 +1324,7 @@ class Executor {
     size_t mark = A_.Mark();
     A_.peak = mark;  // high-water mark of this run
     ctrl_ = (unsigned long long*)A_.Alloc(8 * sizeof(unsigned long long));
+    if (ext_cols_) AllocExternalCache();
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
@@ -1412,6 +1411,9 @@ class Executor {
   uint64_t launches_ = 0, batches_ = 0, paths_ = 0, hot_ = 0, root_h2d_ = 0;
   const uint32_t* ext_cols_ = nullptr;
   uint64_t ext_bytes_ = 0;
+  uint64_t* ext_off_ = nullptr;      // per vertex: list offset in the cache
+  uint32_t* ext_cache_ = nullptr;    // device list cache
+  uint64_t ext_cap_ = 0, ext_used_ = 0, ext_restarts_ = 0;
 
   // Loads, for the paths of Fb, the adjacency lists step `ds` intersects into
   // a device subgraph allocated in the current arena frame (it stays valid
@@ -1425,37 +1427,65 @@ class Executor {
   DGraph LoadSubgraph(const DFront& Fb, const DStep& ds) {
     if (!ext_cols_) return Resident();
     Timed tl = TimerStart();
-    const uint32_t n = (uint32_t)g_.n;
     const size_t mark = A_.Mark();
-    uint8_t* flag = (uint8_t*)A_.Alloc(n);
-    uint64_t* deg = (uint64_t*)A_.Alloc((size_t)n * 8);
-    uint64_t* fl = (uint64_t*)A_.Alloc((size_t)n * 8);
-    CK(cudaMemsetAsync(flag, 0, n, st_));
-    k_ext_mark<<<Grid(Fb.P, 256), 256, 0, st_>>>(Fb, ds, flag);
-    k_ext_deg<<<Grid(n, 256), 256, 0, st_>>>(flag, g_.row_ptrs, n, deg, fl);
-    launches_ += 2;
-    Scan(deg, n);
-    Scan(fl, n);
-    CK(cudaMemcpyAsync(ctx_.h_pinned, deg + n - 1, 8, cudaMemcpyDeviceToHost, st_));
-    CK(cudaMemcpyAsync(ctx_.h_pinned + 1, fl + n - 1, 8, cudaMemcpyDeviceToHost, st_));
-    CK(cudaStreamSynchronize(st_));
-    const uint64_t sub_m = ctx_.h_pinned[0], nid = ctx_.h_pinned[1];
-    // keep the subgraph below the scratch: release the scratch by rebuilding
-    // the frame as [sub_rp, sub_cols, ids] and recomputing from the scans
-    uint64_t* deg_keep = deg;
-    uint64_t* fl_keep = fl;
-    uintE* sub_rp = (uintE*)A_.Alloc((size_t)(n + 1) * 8);
-    uint32_t* sub_cols = (uint32_t*)A_.Alloc(std::max<uint64_t>(sub_m, 1) * 4);
-    uint32_t* ids = (uint32_t*)A_.Alloc(std::max<uint64_t>(nid, 1) * 4);
-    k_ext_rowptr<<<Grid(n + 1, 256), 256, 0, st_>>>(deg_keep, n, sub_rp);
-    k_ext_ids<<<Grid(n, 256), 256, 0, st_>>>(flag, fl_keep, n, ids);
-    k_ext_gather<<<WarpGrid(nid), WARP_BLOCK, 0, st_>>>(ids, (uint32_t)nid, g_.row_ptrs, ext_cols_, sub_rp,
-                                                         sub_cols);
-    launches_ += 3;
-    ext_bytes_ += sub_m * 4;
+    uint32_t* newids = (uint32_t*)A_.Alloc(std::max<size_t>((size_t)Fb.P * std::max<int>(ds.nconn, 1), 1) * 4);
+    unsigned int* nnew = (unsigned int*)A_.Alloc(sizeof(unsigned int));
+    uint64_t total = 0;
+    uint32_t K = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      CK(cudaMemsetAsync(nnew, 0, sizeof(unsigned int), st_));
+      k_ext_claim<<<Grid(Fb.P, 256), 256, 0, st_>>>(Fb, ds, g_.row_ptrs, ext_off_, newids, nnew);
+      Launched();
+      K = (uint32_t)ReadU32(nnew);
+      if (K == 0) break;
+      uint64_t* deg = (uint64_t*)A_.Alloc((size_t)K * 8);
+      k_ext_newdeg<<<Grid(K, 256), 256, 0, st_>>>(newids, K, g_.row_ptrs, deg);
+      Launched();
+      Scan(deg, K);
+      total = ReadU64(deg + K - 1);
+      if (ext_used_ + total <= ext_cap_) {
+        k_ext_place<<<Grid(K, 256), 256, 0, st_>>>(newids, K, deg, ext_used_, ext_off_);
+        k_ext_gather<<<WarpGrid(K), WARP_BLOCK, 0, st_>>>(newids, K, g_.row_ptrs, ext_cols_, ext_off_, ext_cache_);
+        launches_ += 2;
+        ext_used_ += total;
+        ext_bytes_ += total * 4;
+        break;
+      }
+      if (attempt == 1)
+        Fail(SME_ERR_OOM, "external mode: the lists one batch reads (" + std::to_string(total * 4) +
+                              " bytes) exceed the device list cache (" + std::to_string(ext_cap_ * 4) + " bytes)");
+      // the cache is full: start over with this batch's lists
+      CK(cudaMemsetAsync(ext_off_, 0xff, (size_t)(g_.n + 1) * 8, st_));
+      ext_used_ = 0;
+      ++ext_restarts_;
+    }
+    A_.Release(mark);
     TimerStop(tl, kPhaseExternal);
-    (void)mark;
-    return DGraph{sub_rp, sub_cols, nullptr, nullptr, 0};
+    return DGraph{g_.row_ptrs, ext_cache_, nullptr, nullptr, 0, ext_off_};
+  }
+
+  uint64_t ReadU32(const unsigned int* d) {
+    CK(cudaMemcpyAsync(ctx_.h_pinned, d, sizeof(unsigned int), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    return *reinterpret_cast<const unsigned int*>(ctx_.h_pinned);
+  }
+
+  // External mode: the device list cache takes about half of the arena that
+  // is free when the run starts (the frontiers keep the rest).
+  void AllocExternalCache() {
+    ext_off_ = (uint64_t*)A_.Alloc((size_t)(g_.n + 1) * 8);
+    CK(cudaMemsetAsync(ext_off_, 0xff, (size_t)(g_.n + 1) * 8, st_));
+    const uint64_t bytes = std::max<uint64_t>(A_.Free() / 2, 1 << 20) & ~uint64_t(255);
+    ext_cache_ = (uint32_t*)A_.Alloc(bytes);
+    ext_cap_ = bytes / 4;
+    ext_used_ = 0;
+  }
+
+  // Batch cost of an external step in frontier-budget units: the subgraph
+  // bytes count against the list cache (cg scales them so that frontier
+  // bytes / budget + list bytes / cache <= 1).
+  double ExtListCost(uint64_t budget) const {
+    return ext_cols_ && ext_cap_ ? 4.0 * (double)std::max<uint64_t>(budget, 1 << 20) / (double)(ext_cap_ * 4) : 0.0;
   }
   std::vector<Timed> events_;
 
@@ -1700,7 +1730,8 @@ class Executor {
         k_est_compute<<<Grid(F.P, 256), 256, 0, st_>>>(F, ds, g_.row_ptrs, est, sd);
         Launched();
         Scan(sd, F.P);
-        std::vector<Batch> bs = Split(sd, F.P, 0.0, 4.0 + 8.0, Budget(k));
+        const uint64_t bk = Budget(k);
+        std::vector<Batch> bs = Split(sd, F.P, 12.0, 0.0, bk, sd, ExtListCost(bk));
         for (const Batch& b : bs) {
           const size_t mk = A_.Mark();
           DFront Fb = Slice(F, b.b0, b.b1);
@@ -1758,7 +1789,7 @@ class Executor {
     uint64_t budget = Budget(k);
     // keep child counts of a batch within 31-bit path indices
     budget = std::min<uint64_t>(budget, (uint64_t)(std::max(cf, 1.0) * 2.0e9));
-    std::vector<Batch> batches = Split(est, F.P, pf, cf, budget, sumdeg, 4.0 + 8.0);
+    std::vector<Batch> batches = Split(est, F.P, pf, cf, budget, sumdeg, ExtListCost(budget));
     for (const Batch& b : batches) {
       const size_t mark = A_.Mark();
       DFront Fb = Slice(F, b.b0, b.b1);

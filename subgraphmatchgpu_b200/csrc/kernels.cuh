@@ -85,7 +85,17 @@ struct DGraph {
   const int32_t* hub;  // hub slot per vertex, -1 none; null: no bitmaps
   const uint32_t* bm;
   uint32_t words;
+  // external mode: the lists live in a device cache; coff[v] is v's first
+  // element in `cols` (null: cols is the CSR and rp indexes it)
+  const uint64_t* coff;
 };
+
+// Adjacency list of v: its first element and length.
+__device__ __forceinline__ void AdjList(const DGraph& g, uint32_t v, const uint32_t*& ptr, uint32_t& len) {
+  const uint64_t b = __ldg(g.rp + v);
+  len = (uint32_t)(__ldg(g.rp + v + 1) - b);
+  ptr = g.cols + (g.coff ? (len ? __ldg(g.coff + v) : 0) : b);
+}
 
 __device__ __forceinline__ const uint32_t* HubBitmap(const DGraph& g, uint32_t v) {
   if (!g.hub) return nullptr;

@@ -141,7 +141,9 @@ def test_reuse_plan_locates_sibling_caches(graphs, golden, q):
     assert g.count(q, sme.GPU_GPSM_REUSE) == want
     hits = sme.last_stats().reuse_hits
     assert hits > 0
-    assert g.count(q, sme.GPU_GPSM_REUSE, mem_limit_bytes=4 << 20) == want
+    # six-vertex patterns need a larger arena for one path's level buffers
+    budget = (4 << 20) if q in (9, 10) else (8 << 20)
+    assert g.count(q, sme.GPU_GPSM_REUSE, mem_limit_bytes=budget) == want
     assert sme.last_stats().batches > 1
     for name2 in ("ba_n600_m4", "er_n64_d12", "k12"):
         w = golden[name2]["counts"].get(str(q))
