@@ -482,7 +482,10 @@ def bench_batched(args, device):
     return {"graphs": len(gs), "instances": total,
             "batched": {"value": total / (ms / 1e3), "unit": UNIT, "ms": ms, "prepare_autotune_s": prep_s,
                         "group_threads": d["group_threads"], "block_threads": d["block_threads"],
-                        "work_items": d["work_items"], "cuda_graph": True},
+                        "items_per_fetch": d["items_per_fetch"], "tuned_ms": d["tuned_ms"],
+                        "work_items": d["work_items"], "cuda_graph": True,
+                        "tuner": "group of 4/8/16 lanes, a warp, or 64/128 threads of a CTA per item x block "
+                                 "128/256/512, then 1/4/16 items per fetch"},
             "plain": {"value": total / plain_s, "unit": UNIT, "ms": plain_s * 1e3},
             "counts_equal_plain": ok_plain, "counts_equal_cpu": not bad, "cpu_checked_graphs": len(gs),
             "cpu_mismatches": bad[:8], "cpu_check_s": round(cpu_s, 2)}

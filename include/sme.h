@@ -265,7 +265,8 @@ sme_status sme_plan_describe(int32_t query_type, int32_t plan_type, char* buf,
 typedef struct sme_batch_opts {
   int32_t device;
   int32_t autotune;        /* 1: pick granularity/block shape by measuring   */
-  int32_t granularity;     /* 0 auto, 1 warp per root, 2 CTA per root        */
+  int32_t granularity;     /* without autotuning: 0 eight lanes, 1 a warp,
+                              2 a CTA group of 128 threads per root item     */
   int32_t block_threads;   /* 0 auto                                         */
   int32_t use_graph;       /* 1: capture the launch in a CUDA graph          */
   int32_t reserved[11];
@@ -282,6 +283,14 @@ sme_status sme_batch_prepare(sme_graph* const* graphs, const int32_t* queries,
 sme_status sme_batch_run(sme_batch_plan* p, uint64_t* counts, double* ms);
 sme_status sme_batch_describe(const sme_batch_plan* p, int32_t* granularity,
                               int32_t* block_threads, uint64_t* work_items);
+/* The configuration the autotuner kept: threads per group (4, 8, 16 lanes of
+ * a warp, 32 a warp, 64 or 128 warps of a CTA working on one item), threads
+ * per block, work items a group takes per fetch, and its measured time on
+ * the batch (0 without autotuning).  No counterpart in the reference: the
+ * batched form is new. */
+sme_status sme_batch_tuning(const sme_batch_plan* p, int32_t* group_threads,
+                            int32_t* block_threads, int32_t* items_per_fetch,
+                            double* tuned_ms);
 sme_status sme_batch_free(sme_batch_plan* p);
 
 /* Allocation-free count of query `query_type` on one graph whose CSR the

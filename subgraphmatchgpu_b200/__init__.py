@@ -127,6 +127,8 @@ SIGNATURES = {
     "sme_batch_prepare": (C.c_int, [_P, _P, _U64, C.POINTER(BatchOpts), _PP]),
     "sme_batch_run": (C.c_int, [_P, _P, C.POINTER(C.c_double)]),
     "sme_batch_describe": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _PU64]),
+    "sme_batch_tuning": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_double)]),
     "sme_batch_free": (C.c_int, [_P]),
     "sme_count_noalloc": (C.c_int, [_P, _P, _U64, C.c_int32, _PU64]),
     "sme_server_opts_default": (C.c_int, [C.POINTER(ServerOpts)]),
@@ -380,7 +382,10 @@ class BatchPlan:
     def describe(self):
         g, b, n = C.c_int32(), C.c_int32(), C.c_uint64()
         _check(lib().sme_batch_describe(self._h, C.byref(g), C.byref(b), C.byref(n)))
-        return {"group_threads": g.value, "block_threads": b.value, "work_items": n.value}
+        c, ms = C.c_int32(), C.c_double()
+        _check(lib().sme_batch_tuning(self._h, None, None, C.byref(c), C.byref(ms)))
+        return {"group_threads": g.value, "block_threads": b.value, "work_items": n.value,
+                "items_per_fetch": c.value, "tuned_ms": ms.value}
 
     def close(self):
         if self._h and self._h.value:

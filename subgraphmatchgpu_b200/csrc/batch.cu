@@ -70,25 +70,79 @@ struct BArgs {
   uint32_t* scratch;     // per group: nbuf * cap uint32
   uint32_t cap;          // max degree in the batch
   uint32_t nbuf;
+  uint32_t chunk;        // work items a group takes per fetch
 };
 
+// A thread group of G lanes that runs one work item: a part of a warp
+// (G = 4..32, warp intrinsics) or several warps of a CTA (G = 64, 128: the
+// CTA granularity; named barrier 1 + group index, ballot counts exchanged in
+// shared memory).  All lanes of a group follow the same control flow.
+constexpr int kMaxGroupWarps = 4;  // G <= 128
 template <int G>
 struct Tile {
   int lane;            // lane within the group
-  unsigned mask;       // lanes of this group within the warp
-  int base;            // first lane of the group in the warp
-  __device__ Tile() {
-    int l = threadIdx.x & 31;
-    lane = l % G;
-    base = l - lane;
-    mask = (G == 32) ? FULL : (((1u << G) - 1) << base);
+  unsigned mask;       // lanes of this group within the warp (G <= 32)
+  int base;            // first lane of the group in the warp (G <= 32)
+  uint32_t* xs;        // G > 32: this group's exchange words in shared memory
+  int bar;             // G > 32: named barrier of the group
+  __device__ explicit Tile(uint32_t* shared = nullptr) {
+    if constexpr (G <= 32) {
+      int l = threadIdx.x & 31;
+      lane = l % G;
+      base = l - lane;
+      mask = (G == 32) ? FULL : (((1u << G) - 1) << base);
+      xs = nullptr;
+      bar = 0;
+    } else {
+      lane = threadIdx.x % G;
+      base = 0;
+      mask = FULL;
+      const int grp = threadIdx.x / G;
+      xs = shared + grp * (kMaxGroupWarps + 1);
+      bar = 1 + grp;
+    }
   }
-  __device__ unsigned ballot(bool b) const { return (__ballot_sync(mask, b) & mask) >> base; }
-  __device__ uint32_t bcast(uint32_t v) const { return __shfl_sync(mask, v, base); }
-  __device__ unsigned long long sum(unsigned long long v) const {
+  __device__ void sync() const {
+    if constexpr (G > 32) asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(G) : "memory");
+  }
+  // Writes of the group's lanes become visible to the whole group.
+  __device__ void publish() const {
+    if constexpr (G <= 32) __syncwarp(mask);
+    else sync();
+  }
+  __device__ uint32_t bcast(uint32_t v) const {
+    if constexpr (G <= 32) {
+      return __shfl_sync(mask, v, base);
+    } else {
+      if (lane == 0) xs[kMaxGroupWarps] = v;
+      sync();
+      const uint32_t r = xs[kMaxGroupWarps];
+      sync();
+      return r;
+    }
+  }
+  // Number of lanes before this one whose `ok` holds; *total = all of them.
+  __device__ uint32_t rank(bool ok, uint32_t* total) const {
+    if constexpr (G <= 32) {
+      const unsigned m = (__ballot_sync(mask, ok) & mask) >> base;
+      *total = __popc(m);
+      return __popc(m & ((1u << lane) - 1));
+    } else {
+      const unsigned m = __ballot_sync(FULL, ok);
+      const int w = lane >> 5, l = lane & 31;
+      if (l == 0) xs[w] = __popc(m);
+      sync();
+      uint32_t before = 0, tot = 0;
 #pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_down_sync(mask, v, o, G);
-    return v;
+      for (int k = 0; k < G / 32; ++k) {
+        const uint32_t c = xs[k];
+        before += k < w ? c : 0;
+        tot += c;
+      }
+      sync();  // the words are rewritten by the next call
+      *total = tot;
+      return before + __popc(m & ((1u << l) - 1));
+    }
   }
 };
 
@@ -181,30 +235,39 @@ __device__ uint32_t LevelSet(const Tile<G>& t, const BLevel& L, const uint32_t* 
         ok = pos < N[j] && __ldg(A[j] + pos) == x;
       }
     }
-    unsigned m = t.ballot(ok);
-    if (out && ok) out[written + __popc(m & ((1u << t.lane) - 1))] = x;
-    written += __popc(m);
+    uint32_t total;
+    const uint32_t r = t.rank(ok, &total);
+    if (out && ok) out[written + r] = x;
+    written += total;
   }
   if (cnt) {
     unsigned long long c = written;
     *cnt += pair_count ? (c > 0 ? c * (c - 1) / 2 : 0) : c;
   }
+  if (out) t.publish();  // the set is read by every lane of the group next
   if (view) *view = out;
   return written;
 }
 
+// Groups take `a.chunk` consecutive items per fetch (heaviest first): fewer
+// atomics on the shared counter against a coarser balance at the tail.
 template <int G>
 __global__ void k_batch(BArgs a) {
-  Tile<G> t;
+  __shared__ uint32_t xs_sh[16 * (kMaxGroupWarps + 1)];
+  Tile<G> t(xs_sh);
   const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t gid = blockIdx.x * groups_per_block + threadIdx.x / G;
   uint32_t* scratch = a.scratch + (size_t)gid * a.nbuf * a.cap;
+  uint32_t it = 0, it_end = 0;
   while (true) {
-    uint32_t it = 0;
-    if (t.lane == 0) it = atomicAdd(a.next, 1u);
-    it = t.bcast(it);
-    if (it >= a.nitems) break;
-    const uint64_t item = a.items[it];
+    if (it == it_end) {
+      uint32_t first = 0;
+      if (t.lane == 0) first = atomicAdd(a.next, a.chunk);
+      it = t.bcast(first);
+      if (it >= a.nitems) break;
+      it_end = (uint32_t)min((uint64_t)it + a.chunk, a.nitems);
+    }
+    const uint64_t item = a.items[it++];
     const uint32_t g = (uint32_t)(item >> 32);
     const uint32_t root = (uint32_t)item;
     const BProg& P = c_prog[a.query[g]];
@@ -508,7 +571,8 @@ struct sme_batch_plan {
   uint64_t* d_items = nullptr;
   unsigned long long* d_counts = nullptr;
   unsigned int* d_next = nullptr;
-  int G = 8, block = 256, grid = 0;
+  int G = 8, block = 256, grid = 0, chunk = 1;
+  float tuned_ms = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
@@ -539,6 +603,7 @@ BArgs Args(sme_batch_plan* p) {
   a.scratch = p->d_scratch;
   a.cap = p->cap;
   a.nbuf = p->nbuf;
+  a.chunk = (uint32_t)std::max(1, p->chunk);
   return a;
 }
 
@@ -556,6 +621,8 @@ void Launch(sme_batch_plan* p, int G, int block, int grid) {
     case 4: k_batch<4><<<grid, block, 0, p->stream>>>(a); break;
     case 8: k_batch<8><<<grid, block, 0, p->stream>>>(a); break;
     case 16: k_batch<16><<<grid, block, 0, p->stream>>>(a); break;
+    case 64: k_batch<64><<<grid, block, 0, p->stream>>>(a); break;
+    case 128: k_batch<128><<<grid, block, 0, p->stream>>>(a); break;
     default: k_batch<32><<<grid, block, 0, p->stream>>>(a); break;
   }
 }
@@ -566,6 +633,8 @@ int GridFor(sme_batch_plan* p, int G, int block) {
     case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<4>, block, 0); break;
     case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<8>, block, 0); break;
     case 16: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<16>, block, 0); break;
+    case 64: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<64>, block, 0); break;
+    case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<128>, block, 0); break;
     default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_batch<32>, block, 0); break;
   }
   return std::max(1, blocks_per_sm) * SmCountB(p->device);
@@ -654,16 +723,27 @@ void Prepare(sme_graph* const* graphs, const int32_t* queries, uint64_t num, con
   BCK(cudaMalloc((void**)&p->d_counts, num * sizeof(unsigned long long)));
   BCK(cudaMalloc((void**)&p->d_next, sizeof(unsigned int)));
   // scratch for the largest grid of any candidate configuration
+  static const int kGroups[] = {4, 8, 16, 32, 64, 128};
+  static const int kBlocks[] = {128, 256, 512};
   int max_groups = 0;
-  for (int G : {4, 8, 16, 32})
-    for (int block : {128, 256, 512}) max_groups = std::max(max_groups, GridFor(p, G, block) * (block / G));
+  for (int G : kGroups)
+    for (int block : kBlocks)
+      if (block >= G) max_groups = std::max(max_groups, GridFor(p, G, block) * (block / G));
   BCK(cudaMalloc((void**)&p->d_scratch, (size_t)max_groups * p->nbuf * p->cap * 4));
-  // autotune: time each candidate on the batch itself
-  int bestG = o.granularity == 2 ? 32 : 8, bestB = o.block_threads ? o.block_threads : 256;
+  // autotune on the batch itself: group size (a part of a warp, a warp, or
+  // two or four warps of a CTA) x block shape with one item per fetch, then
+  // the items per fetch for the winner
+  int bestG = o.granularity == 2 ? 128 : o.granularity == 1 ? 32 : 8;
+  int bestB = o.block_threads ? o.block_threads : 256;
+  if (bestB < bestG) bestB = bestG;
+  int bestC = 1;
+  float best = 0;
   if (o.autotune) {
-    float best = 1e30f;
-    for (int G : {4, 8, 16, 32})
-      for (int block : {128, 256, 512}) {
+    best = 1e30f;
+    p->chunk = 1;
+    for (int G : kGroups)
+      for (int block : kBlocks) {
+        if (block < G) continue;
         float ms = TimeConfig(p, G, block);
         if (ms < best) {
           best = ms;
@@ -671,9 +751,19 @@ void Prepare(sme_graph* const* graphs, const int32_t* queries, uint64_t num, con
           bestB = block;
         }
       }
+    for (int c : {4, 16}) {
+      p->chunk = c;
+      float ms = TimeConfig(p, bestG, bestB);
+      if (ms < best) {
+        best = ms;
+        bestC = c;
+      }
+    }
   }
   p->G = bestG;
   p->block = bestB;
+  p->chunk = bestC;
+  p->tuned_ms = best;
   p->grid = GridFor(p, bestG, bestB);
   if (p->use_graph) {
     BCK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
@@ -762,6 +852,16 @@ sme_status sme_batch_describe(const sme_batch_plan* p, int32_t* g, int32_t* bloc
   if (g) *g = p->G;
   if (block) *block = p->block;
   if (items) *items = p->nitems;
+  return SME_OK;
+}
+
+sme_status sme_batch_tuning(const sme_batch_plan* p, int32_t* group_threads, int32_t* block_threads,
+                            int32_t* items_per_fetch, double* tuned_ms) {
+  if (!p) return SME_ERR_INVALID_ARG;
+  if (group_threads) *group_threads = p->G;
+  if (block_threads) *block_threads = p->block;
+  if (items_per_fetch) *items_per_fetch = p->chunk;
+  if (tuned_ms) *tuned_ms = p->tuned_ms;
   return SME_OK;
 }
 

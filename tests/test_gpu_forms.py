@@ -61,16 +61,19 @@ def test_batched_form_matches_oracle_per_graph():
     got2, _ = plan.run()  # graph replay
     assert np.array_equal(got2, want)
     d = plan.describe()
-    assert d["group_threads"] in (4, 8, 16, 32) and d["work_items"] == sum(g.n for g in gs)
+    assert d["group_threads"] in (4, 8, 16, 32, 64, 128) and d["work_items"] == sum(g.n for g in gs)
+    assert d["items_per_fetch"] in (1, 4, 16) and d["tuned_ms"] > 0
 
 
-@pytest.mark.parametrize("gran,block", [(1, 128), (2, 256)])
+@pytest.mark.parametrize("gran,block", [(0, 128), (1, 128), (2, 256), (2, 128)])
 def test_batched_form_fixed_configurations(gran, block):
+    # 0: eight lanes, 1: a warp, 2: a CTA group of 128 threads per item
     gs, qs = small_graphs(40, 9)
     want = np.array([O.count(*g.csr(), q) for g, q in zip(gs, qs)], dtype=np.uint64)
     plan = sme.BatchPlan(gs, qs, autotune=False, use_graph=False, granularity=gran, block_threads=block)
     got, _ = plan.run()
     assert np.array_equal(got, want)
+    assert plan.describe()["group_threads"] == {0: 8, 1: 32, 2: 128}[gran]
 
 
 def test_batched_form_all_queries():
