@@ -81,6 +81,9 @@ def parse(argv=None):
     ap.add_argument("--no-s22", action="store_true", help="skip the R-MAT s22 legs")
     ap.add_argument("--no-l2-flush", action="store_true", help="do not flush L2 between steps")
     ap.add_argument("--threads", type=int, default=0, help="CPU threads (0: all)")
+    ap.add_argument("--profile-s22", default="",
+                    help="BEGIN:END: only count the 4-clique of the degree-oriented R-MAT s22 graph over roots "
+                         "[BEGIN, END) once (a small case for a profiler capture), print its stats and exit")
     return ap.parse_args(argv)
 
 
@@ -682,6 +685,24 @@ def bench_s22(args, device, tune, peak):
     return out
 
 
+def profile_s22(args):
+    """One count of the 4-clique over a root range of the degree-oriented
+    R-MAT s22 ef16 graph (the graph of the s22 legs), resident, with the
+    device footprint kept small: the case a profiler capture replays."""
+    import subgraphmatchgpu_b200 as sme
+    b, e = (int(x) for x in args.profile_s22.split(":"))
+    g = sme.Graph.rmat(22, args.edge_factor, 0.57, 0.19, 0.19, seed=22)
+    o, _ = g.degree_order(orient=True)
+    del g
+    o.to_device(0)
+    c = o.count(3, args.algo, root_begin=b, root_end=e, mem_limit_bytes=2 << 30,
+                warp_granularity=args.granularity)
+    s = sme.last_stats()
+    print(json.dumps({"roots": [b, e], "instances": c, "device_ms": s.device_ms, "kernel_ms": s.kernel_ms,
+                      "algorithmic_bytes": s.algorithmic_bytes, "launches": s.kernel_launches,
+                      "hot_launches": s.hot_launches, "phase_ms": list(s.phase_ms)}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -689,6 +710,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.profile_s22:
+        return profile_s22(args)
 
     import torch
     import subgraphmatchgpu_b200 as sme

@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     uint64_t out_off = 0;
     if (MODE == 0) {
       out_off = (p + b0 == 0 ? 0 : est_incl[p + b0 - 1]) - base;
-      if (nl == 1) {
+      if (nl == 1 && !s.noview) {
         // single list: the candidate set is a sub-range unless an excluded
         // value falls inside it
         uint32_t ex[MAXV];
@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute_flat(
       if (nl > 0) Range(L[0], N[0], bd, r0, r1);
       if (MODE == 0) {
         fp.out_off = (p + b0 == 0 ? 0 : est_incl[p + b0 - 1]) - base;
-        if (nl == 1) {
+        if (nl == 1 && !s.noview) {
           uint32_t ex[MAXV];
           if (Exclusions(L[0], r0, r1, bd, ex) == 0) {
             out_ptr[p] = (uint64_t)(L[0] + r0);
@@ -1713,7 +1713,8 @@ class Executor {
       return;
     }
     const Step& s = prog_.steps[k];
-    const DStep ds = ToDStep(s);
+    DStep ds = ToDStep(s);
+    ds.noview = ext_cols_ != nullptr;
     unsigned long long* acc = ctrl_;
     uint32_t* err = (uint32_t*)(ctrl_ + 3);
     switch (s.kind) {

@@ -65,6 +65,9 @@ struct DStep {
   uint8_t mx;
   uint8_t mmask;
   uint8_t mop;  // level 1's order against M[0] the sibling's vertex obeys (0 <, 1 >, else none)
+  // 1: a single-list set is copied, never a view into the list (external
+  // mode: the list cache is reused by later batches while the set lives on)
+  uint8_t noview;
 };
 
 struct DMatOut {

@@ -37,6 +37,21 @@ def test_external_mode_small_budget_loads_many_subgraphs(golden):
         assert 8 * (n + 1) < s.h2d_bytes <= 8 * (n + 1) + 4 * m
 
 
+def test_external_mode_restarts_its_list_cache():
+    # R-MAT s16 ef16 holds ~7 MB of lists; an 8 MiB budget leaves the list
+    # cache about half of that, so it fills and starts over many times while
+    # sets computed earlier (copies, never views into the cache) live on
+    g = sme.Graph.rmat(16, 16, seed=3)
+    n, m, _ = g.info()
+    assert 4 * m > 6 << 20
+    for q in (0, 3, 2, 1):
+        want = g.count(q, sme.GPU_LIGHT, root_stride=7 if q == 1 else 1)
+        got = g.count(q, sme.GPU_LIGHT, sme.EXTERNAL_GPU, mem_limit_bytes=8 << 20, root_stride=7 if q == 1 else 1)
+        assert got == want, q
+        s = sme.last_stats()
+        assert s.batches > 2 and s.h2d_bytes > 8 * (n + 1)
+
+
 def small_graphs(num, seed):
     rnd = random.Random(seed)
     gs, qs = [], []
