@@ -1162,14 +1162,21 @@ __global__ void k_build_bitmaps(const uintE* __restrict__ rp, const uint32_t* __
 }
 
 // Bitmaps for the vertices of highest degree (>= kHubMinDegree) within a
-// byte budget (SME_HUB_BITMAP_MB, default 256 MiB); a bitmap is n bits.
-// `alloc` hands out device memory (cudaMalloc, or the context's arena for a
-// per-call upload); `scratch_owned` frees the temporary hub list afterwards.
+// byte budget (SME_HUB_BITMAP_MB, default 1 GiB, at most a quarter of the
+// device memory `room` the caller can spare); a bitmap is n bits.  Measured
+// on R-MAT s20 (root blocks of the bench): 256 MiB 9.5e9, 512 MiB 9.8e9,
+// 1 GiB 10.5e9, 2 GiB 10.7e9 instances/s, flat beyond; whole-graph counts
+// flat from 512 MiB.  `alloc` hands out device memory (cudaMalloc, or the
+// context's arena for a per-call upload); `scratch_owned` frees the
+// temporary hub list afterwards.
 template <typename Alloc>
-void BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream, Alloc alloc, bool scratch_owned) {
-  const uint64_t kHubMinDegree = 256;
-  uint64_t budget = 256ULL << 20;
+void BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream, Alloc alloc, bool scratch_owned,
+                     uint64_t room) {
+  uint64_t kHubMinDegree = 256;
+  if (const char* e = std::getenv("SME_HUB_MIN_DEGREE")) kHubMinDegree = std::strtoull(e, nullptr, 10);
+  uint64_t budget = 1024ULL << 20;
   if (const char* e = std::getenv("SME_HUB_BITMAP_MB")) budget = std::strtoull(e, nullptr, 10) << 20;
+  budget = std::min<uint64_t>(budget, room / 4);
   const uint32_t words = (uint32_t)((g.n + 31) / 32);
   if (budget == 0 || words == 0) return;
   const uint64_t max_hubs = budget / ((uint64_t)words * 4);
@@ -1220,7 +1227,9 @@ DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, ui
       CK(cudaMalloc(&p, bytes));
       return p;
     };
-    BuildHubBitmaps(d, g, stream, dev_alloc, true);
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    BuildHubBitmaps(d, g, stream, dev_alloc, true, fr);
   } catch (...) {
     FreeDeviceGraph(d);
     throw;
@@ -1242,7 +1251,7 @@ DeviceGraph* UploadGraphToArena(const HostGraph& g, DeviceContext& ctx, uint64_t
     d->cols = (uintV*)arena_alloc(std::max<uint64_t>(g.m, 1) * sizeof(uintV));
     CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, ctx.stream));
     if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, ctx.stream));
-    BuildHubBitmaps(d, g, ctx.stream, arena_alloc, false);
+    BuildHubBitmaps(d, g, ctx.stream, arena_alloc, false, ctx.arena.Free());
     CK(cudaStreamSynchronize(ctx.stream));
   } catch (...) {
     delete d;
