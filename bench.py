@@ -82,8 +82,9 @@ def parse(argv=None):
     ap.add_argument("--no-l2-flush", action="store_true", help="do not flush L2 between steps")
     ap.add_argument("--threads", type=int, default=0, help="CPU threads (0: all)")
     ap.add_argument("--profile-s22", default="",
-                    help="BEGIN:END: only count the 4-clique of the degree-oriented R-MAT s22 graph over roots "
-                         "[BEGIN, END) once (a small case for a profiler capture), print its stats and exit")
+                    help="BEGIN:END:STRIDE: only count the 4-clique of the degree-oriented R-MAT s22 graph over "
+                         "roots BEGIN, BEGIN+STRIDE, ... < END once (a small case for a profiler capture), print "
+                         "its stats and exit")
     return ap.parse_args(argv)
 
 
@@ -690,15 +691,15 @@ def profile_s22(args):
     R-MAT s22 ef16 graph (the graph of the s22 legs), resident, with the
     device footprint kept small: the case a profiler capture replays."""
     import subgraphmatchgpu_b200 as sme
-    b, e = (int(x) for x in args.profile_s22.split(":"))
+    b, e, st = (int(x) for x in args.profile_s22.split(":"))
     g = sme.Graph.rmat(22, args.edge_factor, 0.57, 0.19, 0.19, seed=22)
     o, _ = g.degree_order(orient=True)
     del g
     o.to_device(0)
-    c = o.count(3, args.algo, root_begin=b, root_end=e, mem_limit_bytes=2 << 30,
+    c = o.count(3, args.algo, root_begin=b, root_end=e, root_stride=st, mem_limit_bytes=2 << 30,
                 warp_granularity=args.granularity)
     s = sme.last_stats()
-    print(json.dumps({"roots": [b, e], "instances": c, "device_ms": s.device_ms, "kernel_ms": s.kernel_ms,
+    print(json.dumps({"roots": [b, e, st], "instances": c, "device_ms": s.device_ms, "kernel_ms": s.kernel_ms,
                       "algorithmic_bytes": s.algorithmic_bytes, "launches": s.kernel_launches,
                       "hot_launches": s.hot_launches, "phase_ms": list(s.phase_ms)}), flush=True)
 
@@ -816,6 +817,7 @@ def main():
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
                 "kernel": "intersection kernels (COMPUTE / COMPUTE_COUNT / COMPUTE_PATH_COUNT)",
                 "algorithmic_bytes_per_launch": alg_per_launch, "avg_launch_ms": kern_ms / max(hot, 1),
+                "launches": hot,
                 "bytes_definition": "per path: 12 per backward list (row pointers + gathered vertex) + 4 x clipped "
                                     "pivot length x lists intersected + 4 per candidate written",
                 "traffic": traffic,
