@@ -823,7 +823,12 @@ def main():
                 "traffic": traffic,
                 "dram_achieved_gbs": (round(traffic / (kern_ms / max(hot, 1) / 1e3) / 1e9, 1)
                                       if traffic and kern_ms > 0 else None),
-                "traffic_source": tr.get("source") if tr else None}
+                "dram_frac": (round(traffic / (kern_ms / max(hot, 1) / 1e3) / 1e9 / peak, 4)
+                              if traffic and kern_ms > 0 else None),
+                "traffic_source": tr.get("source") if tr else None,
+                "note": "achieved/frac count the bytes the probe-based intersection must touch (4 per probed "
+                        "word); DRAM moves 32-byte sectors, so physical traffic (traffic, dram_achieved_gbs, "
+                        "dram_frac) is the ncu-measured multiple of them"}
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
