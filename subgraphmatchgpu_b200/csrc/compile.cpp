@@ -60,6 +60,7 @@ const char* KindName(StepKind k) {
     case S_COMPUTE_COUNT: return "COMPUTE_COUNT";
     case S_PATH_COUNT: return "COMPUTE_PATH_COUNT";
     case S_COUNT: return "COUNT";
+    case S_ALIAS: return "ALIAS";
   }
   return "?";
 }
@@ -476,6 +477,33 @@ Program CompileLight(const Query& q, int compress_level, bool enumerate, bool se
 // candidates of a root are all of N(M[0]) in order (COMPUTE(1) over {0}
 // with no condition, MATERIALIZE(1) with none) and the level-2 cache is the
 // plain intersection N(M[0]) ∩ N(M[1]); otherwise the step keeps its lists.
+// A COMPUTE or COMPUTE_PATH_COUNT that repeats an earlier step of the same
+// kind (same lists, reused set and conditions) while that step's set is
+// still live computes the same set for every path: it becomes an alias of
+// that set.  The diamond's LIGHT plan counts N(u0) ∩ N(u2) twice
+// (COMPUTE_PATH_COUNT for u1 and for u3, LazyTraversalPlanGenerator.h:266-274);
+// the second is now free.
+static void AliasRepeatedComputes(Program& p) {
+  for (size_t k = 1; k < p.steps.size(); ++k) {
+    Step& s = p.steps[k];
+    if ((s.kind != S_COMPUTE && s.kind != S_PATH_COUNT) || s.with_u >= 0 || s.map_src >= 0) continue;
+    const std::vector<uint8_t>& live = p.steps[k - 1].sets_after;
+    for (size_t j = 0; j < k; ++j) {
+      const Step& e = p.steps[j];
+      if (e.kind != s.kind || e.conn != s.conn || e.reuse_src != s.reuse_src || e.map_src >= 0 ||
+          std::find(live.begin(), live.end(), e.u) == live.end())
+        continue;
+      bool same = e.cond.size() == s.cond.size();
+      for (size_t i = 0; same && i < s.cond.size(); ++i)
+        same = e.cond[i].op == s.cond[i].op && e.cond[i].operand == s.cond[i].operand;
+      if (!same) continue;
+      s.kind = S_ALIAS;
+      s.alias_of = (int8_t)e.u;
+      break;
+    }
+  }
+}
+
 static void RequireSiblingLayout(Program& p) {
   auto find = [&](StepKind k, uint8_t u) -> const Step* {
     for (const Step& s : p.steps)
@@ -529,6 +557,7 @@ Program Compile(const sme_opts& o, bool enumerate, bool loop_free) {
   p.enumerate = enumerate;
   PruneImpliedExclusions(p, loop_free);
   RequireSiblingLayout(p);
+  if (!enumerate) AliasRepeatedComputes(p);
   for (auto& s : p.steps) {
     std::ostringstream os;
     os << KindName(s.kind) << "(" << (int)s.u << ")";
@@ -586,6 +615,7 @@ std::string Program::Describe() const {
       os << ")";
     }
     if (s.with_u >= 0) os << " with=" << (int)s.with_u;
+    if (s.kind == S_ALIAS) os << " of=" << (int)s.alias_of;
     if (s.kind == S_COUNT) os << (s.direct ? " direct" : " general");
     if (s.keep_set) os << " keep";
     os << " | mat=(";

@@ -200,6 +200,57 @@ __global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __res
   }
 }
 
+// ---- paths grouped by the hub they probe ------------------------------------
+// A count step's membership tests land on the dense bitmap of the hub whose
+// list is searched.  Taken in frontier order, consecutive paths probe
+// different hubs and every 4-byte test pulls a 32-byte sector from DRAM (the
+// bitmaps do not fit L2); taken hub by hub, a hub's bitmap stays in L2 while
+// its paths run.  A counting sort by hub slot (non-hubs in one last bucket)
+// gives the order: warp-aggregated counts, a scan, a warp-aggregated scatter.
+__global__ void k_hub_hist(DFront F, uint8_t kv, const int32_t* __restrict__ hub, uint32_t nb,
+                           unsigned long long* cnt) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = w0; base < F.P; base += stride) {
+    const uint32_t p = base + lane;
+    uint32_t key = 0xffffffffu;
+    if (p < F.P) {
+      const int32_t h = __ldg(hub + F.inst[kv][p]);
+      key = h < 0 ? nb - 1 : (uint32_t)h;
+    }
+    const unsigned same = __match_any_sync(FULL, key);
+    if (key != 0xffffffffu && lane == __ffs(same) - 1) atomicAdd(cnt + key, (unsigned long long)__popc(same));
+  }
+}
+
+__global__ void k_hub_cursor(const unsigned long long* __restrict__ incl, const unsigned long long* cnt,
+                             uint32_t nb, unsigned long long* cur) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+    cur[b] = incl[b] - cnt[b];
+}
+
+__global__ void k_hub_scatter(DFront F, uint8_t kv, const int32_t* __restrict__ hub, uint32_t nb,
+                              unsigned long long* cur, uint32_t* perm) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = w0; base < F.P; base += stride) {
+    const uint32_t p = base + lane;
+    uint32_t key = 0xffffffffu;
+    if (p < F.P) {
+      const int32_t h = __ldg(hub + F.inst[kv][p]);
+      key = h < 0 ? nb - 1 : (uint32_t)h;
+    }
+    const unsigned same = __match_any_sync(FULL, key);
+    const int leader = __ffs(same) - 1;
+    unsigned long long at = 0;
+    if (key != 0xffffffffu && lane == leader) at = atomicAdd(cur + key, (unsigned long long)__popc(same));
+    at = __shfl_sync(FULL, at, leader);
+    if (key != 0xffffffffu) perm[at + __popc(same & ((1u << lane) - 1))] = p;
+  }
+}
+
 // ---- mapped reuse: the sibling path's cached intersection ----------------
 // In the reuse plan the level-1 paths of a root M[0] are its neighbours N(M[0])
 // in order (one contiguous run per root; the compiler checks level 1 has no
@@ -247,7 +298,8 @@ __device__ __forceinline__ void SiblingSet(const DFront& F, const DStep& s, cons
 // hv.min_len elements is queued for k_compute_cta instead.  MAPPED (reuse
 // plan, s.msrc >= 0): the set cached by the sibling path replaces the lists
 // of s.mmask when the sibling is in the current batch (see SiblingSet).
-template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV, bool DEFER = false, bool MAPPED = false>
+template <int MODE, int MINB = 1, int NLM = MAXV, int NEX = MAXV, bool DEFER = false, bool MAPPED = false,
+          bool PERM = false>
 __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     DFront F, DStep s, DGraph G, const uint64_t* __restrict__ est_incl, uint32_t b0, uint64_t* out_ptr,
     uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc, uint32_t* err,
@@ -259,7 +311,8 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
   unsigned long long local = 0, bytes = 0, hits = 0;
   const uint64_t base = b0 == 0 ? 0 : est_incl[b0 - 1];
 
-  for (uint32_t p = gw; p < F.P; p += nw) {
+  for (uint32_t pi = gw; pi < F.P; pi += nw) {
+    const uint32_t p = PERM ? __ldg(hv.perm + pi) : pi;
     const uint32_t* L[NLM];
     const uint32_t* B[NLM];  // hub bitmap of the list (null: binary search)
     uint32_t N[NLM];
@@ -1506,6 +1559,33 @@ class Executor {
   }
   unsigned WarpGrid(uint64_t paths) const { return Grid(paths * 32, WARP_BLOCK); }
 
+  // The order in which a count step takes its paths: grouped by the hub
+  // slot of the step's last list vertex (the most recently materialised one,
+  // which changes fastest along the frontier), or nullptr to keep the
+  // frontier order (no bitmaps, a small frontier, no room, or turned off).
+  const uint32_t* GroupByHub(const DFront& F, const DStep& ds) {
+    if (!group_by_hub_ || !use_bitmaps_ || !g_.hub_slot || g_.nhubs == 0 || ds.nconn == 0 || F.P < (1u << 16))
+      return nullptr;
+    const uint32_t nb = g_.nhubs + 1;
+    const size_t need = (size_t)F.P * 4 + (size_t)nb * 24 + (((size_t)nb + SCAN_TILE - 1) / SCAN_TILE) * 8 + 4096;
+    if (A_.Free() < need + (16u << 20)) return nullptr;
+    Timed to = TimerStart();
+    const uint8_t kv = ds.conn[ds.nconn - 1];
+    unsigned long long* cnt = (unsigned long long*)A_.Alloc((size_t)nb * 8);
+    unsigned long long* incl = (unsigned long long*)A_.Alloc((size_t)nb * 8);
+    unsigned long long* cur = (unsigned long long*)A_.Alloc((size_t)nb * 8);
+    uint32_t* perm = (uint32_t*)A_.Alloc((size_t)F.P * 4);
+    CK(cudaMemsetAsync(cnt, 0, (size_t)nb * 8, st_));
+    k_hub_hist<<<Grid(F.P, 256), 256, 0, st_>>>(F, kv, g_.hub_slot, nb, cnt);
+    CK(cudaMemcpyAsync(incl, cnt, (size_t)nb * 8, cudaMemcpyDeviceToDevice, st_));
+    Scan(reinterpret_cast<uint64_t*>(incl), nb);
+    k_hub_cursor<<<Grid(nb, 256), 256, 0, st_>>>(incl, cnt, nb, cur);
+    k_hub_scatter<<<Grid(F.P, 256), 256, 0, st_>>>(F, kv, g_.hub_slot, nb, cur, perm);
+    launches_ += 3;
+    TimerStop(to, kPhaseOrganize);
+    return perm;
+  }
+
   // Window of k_compute_cta in dynamic shared memory (64 KiB: two CTAs of
   // 512 threads per SM), the attribute set once per device.
   template <int MODE>
@@ -1549,7 +1629,7 @@ class Executor {
   // warp per path generic (1) or flattened over 32 paths per warp (2).
   template <int MODE>
   void Compute(const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est, uint32_t b0, uint64_t* ptr,
-               uint32_t* cnt, uint32_t* data, uint64_t cap) {
+               uint32_t* cnt, uint32_t* data, uint64_t cap, const uint32_t* perm = nullptr) {
     unsigned long long* acc = ctrl_;
     uint32_t* err = (uint32_t*)(ctrl_ + 3);
     Timed t = TimerStart();
@@ -1557,7 +1637,28 @@ class Executor {
     const int nlists = ds.nconn + (ds.reuse >= 0 ? 1 : 0);
     bool has_ne = false;
     for (int i = 0; i < ds.cond.n; ++i) has_ne |= ds.cond.op[i] == 2;
-    if (ds.msrc >= 0) {
+    if (MODE == 1 && perm && ds.msrc < 0 && (gran == 0 || gran == 3) && nlists <= 3) {
+      // count step, paths taken hub by hub (see k_hub_hist)
+      if constexpr (MODE == 1) {
+        DHeavy hv{};
+        hv.perm = perm;
+        if (nlists <= 2) {
+          if (has_ne)
+            k_compute<1, 8, 2, MAXV, false, false, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
+                F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, hv);
+          else
+            k_compute<1, 8, 2, 0, false, false, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
+                F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, hv);
+        } else {
+          if (has_ne)
+            k_compute<1, 8, 3, MAXV, false, false, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
+                F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, hv);
+          else
+            k_compute<1, 8, 3, 0, false, false, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
+                F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, hv);
+        }
+      }
+    } else if (ds.msrc >= 0) {
       // mapped reuse: the warp kernel that looks up the sibling's set
       if (has_ne)
         k_compute<MODE, 4, MAXV, MAXV, false, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
@@ -1619,6 +1720,7 @@ class Executor {
  public:
   int gran_ = 0;
   uint32_t heavy_min_ = 2048;  // granularity 4: shortest pivot that gets a CTA
+  bool group_by_hub_ = false;  // count steps take their paths hub by hub
   bool use_bitmaps_ = true;
 
  private:
@@ -1730,7 +1832,10 @@ class Executor {
       case S_COMPUTE_COUNT: {
         paths_ += F.P;
         if (!ext_cols_) {
-          Compute<1>(F, ds, Resident(), nullptr, 0, nullptr, nullptr, nullptr, 0);
+          const size_t mg = A_.Mark();
+          const uint32_t* perm = GroupByHub(F, ds);
+          Compute<1>(F, ds, Resident(), nullptr, 0, nullptr, nullptr, nullptr, 0, perm);
+          A_.Release(mg);
           return;
         }
         // external: batches whose required lists fit the level budget
@@ -1751,6 +1856,16 @@ class Executor {
           A_.Release(mk);
         }
         A_.Release(m0);
+        return;
+      }
+      case S_ALIAS: {
+        DFront Fn = F;
+        const int a = s.alias_of;
+        Fn.set[s.u] = F.set[a];
+        Fn.cidx[s.u] = F.cidx[a];
+        Fn.ident_off[s.u] = F.ident_off[a];
+        Fn.nset[s.u] = F.nset[a];
+        Level(k + 1, Fn);
         return;
       }
       case S_COUNT: {
@@ -1904,6 +2019,7 @@ RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& c
   ex.gran_ = tuning & 0xff;
   ex.use_bitmaps_ = !(tuning & 0x100);
   if (const char* e = std::getenv("SME_HEAVY_PIVOT")) ex.heavy_min_ = (uint32_t)std::max(32L, std::atol(e));
+  if (const char* e = std::getenv("SME_GROUP_BY_HUB")) ex.group_by_hub_ = std::atoi(e) != 0;
   return ex.Run(t);
 }
 

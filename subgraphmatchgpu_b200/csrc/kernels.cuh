@@ -27,6 +27,9 @@ struct DHeavy {
   uint32_t* q;
   uint32_t cap;
   uint32_t min_len;
+  // PERM launches: the order in which the paths are taken (path i of the
+  // launch is perm[i]); a count is the same in any order
+  const uint32_t* perm;
 };
 
 struct DSet {

@@ -166,7 +166,8 @@ enum StepKind : uint8_t {
   S_FILTER = 3,        // re-filter u's candidate sets (FILTER_COMPUTE)
   S_COMPUTE_COUNT = 4, // count candidates of u (optionally ranked into with_u)
   S_PATH_COUNT = 5,    // per-path candidate count only (COMPUTE_PATH_COUNT)
-  S_COUNT = 6          // LIGHTCount / LIGHTDirectCount over unmaterialised sets
+  S_COUNT = 6,         // LIGHTCount / LIGHTDirectCount over unmaterialised sets
+  S_ALIAS = 7          // u's set is an earlier step's identical set (no work)
 };
 struct StepCond { uint8_t op; uint8_t operand; };
 struct Step {
@@ -174,6 +175,7 @@ struct Step {
   uint8_t u = 0;
   std::vector<uint8_t> conn;      // materialised vertices: adjacency lists
   int8_t reuse_src = -1;          // vertex whose cached set is intersected
+  int8_t alias_of = -1;           // S_ALIAS: vertex whose live set u shares
   std::vector<uint8_t> full_conn; // fallback when no cache (reuse plan)
   int8_t map_src = -1;            // reuse plan: mapped meta's cached level
   uint8_t map_x = 0;              //   vertex in the sibling's level-1 place
