@@ -81,7 +81,8 @@ typedef struct sme_opts {
                               (Q4), whose search sequence starts at u1      */
   int32_t warp_granularity;/* intersection launch shape: 0 auto (warp per
                               path, specialised on list count, tuned
-                              occupancy), 1 warp per path generic,
+                              occupancy; on an oriented graph, whose lists
+                              are short, as 2), 1 warp per path generic,
                               2 flattened (32 paths per warp), 3 as 0 with
                               six blocks per SM throughout, 4 as 0 with a
                               CTA per path whose clipped pivot is long

@@ -134,7 +134,7 @@ static RunOut Execute(sme_graph* g, const sme_opts& o, bool enumerate, uint32_t*
           Fail(SME_ERR_OOM, "cannot allocate enumeration buffer");
         }
       }
-      r = RunProgram(prog, *dg, ctx, task, d_out, cap, Tuning(o));
+      r = RunProgram(prog, *dg, ctx, task, d_out, cap, TuningFor(o, g->g));
       if (enumerate && cap && host_out) {
         uint64_t ncopy = std::min<uint64_t>(r.emitted, cap);
         if (ncopy) {

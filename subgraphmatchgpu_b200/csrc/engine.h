@@ -85,6 +85,17 @@ RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& c
 // specialised; 1 warp per path generic; 2 flattened, specialised; 3 as 0 at
 // six blocks per SM); bit 8 set = no hub bitmaps.
 inline int Tuning(const sme_opts& o) { return (o.warp_granularity & 0xff) | (o.list_only ? 0x100 : 0); }
+// The launch for a graph: the auto choice (granularity 0) takes the
+// flattened kernel on an oriented graph, whose lists are short (the
+// degree-oriented R-MAT s22 4-clique 2026 -> 1501 ms, 5-clique every 16th
+// root 6772 -> 4391 ms), and the warp per path elsewhere (on R-MAT s20 as
+// generated the flattened kernel is 40-60% slower on the 4-cycle, diamond and
+// house).
+inline int TuningFor(const sme_opts& o, const HostGraph& g) {
+  int t = Tuning(o);
+  if ((t & 0xff) == 0 && g.oriented) t |= 2;
+  return t;
+}
 
 // External (chunked) execution over a graph that stays in host memory.
 RunResult RunProgramExternal(const Program& prog, const HostGraph& g, DeviceContext& ctx, const RootTask& task,

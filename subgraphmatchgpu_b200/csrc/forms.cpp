@@ -140,7 +140,7 @@ struct sme_server {
             dg = UploadGraphToArena(hg, *ctx, nullptr);
             temp = true;
           }
-          rr = RunProgram(prog, *dg, *ctx, TaskOf(r.opts, hg.n), nullptr, 0, Tuning(r.opts));
+          rr = RunProgram(prog, *dg, *ctx, TaskOf(r.opts, hg.n), nullptr, 0, TuningFor(r.opts, hg));
         } catch (...) {
           if (temp) FreeDeviceGraph(dg);
           ctx->arena.Release(graph_mark);
