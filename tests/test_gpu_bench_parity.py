@@ -109,3 +109,15 @@ def test_explicit_root_task_counts_each_listed_root():
     with pytest.raises(sme.SmeError) as e:
         g.count(3, roots=np.array([g.n], np.uint32))
     assert e.value.status == 1
+
+
+def test_count_steps_grouped_by_hub(monkeypatch):
+    # SME_GROUP_BY_HUB=1: a count step takes its paths grouped by the hub
+    # whose bitmap it probes (a counting sort of the frontier); the count is
+    # the same in any order
+    g, _ = engine_graph(16, 16)
+    want = {q: g.count(q, sme.GPU_LIGHT) for q in (3, 2, 1)}
+    monkeypatch.setenv("SME_GROUP_BY_HUB", "1")
+    for q, w in want.items():
+        assert g.count(q, sme.GPU_LIGHT) == w, q
+        assert g.count(q, sme.GPU_GPSM) == w, q
