@@ -171,7 +171,11 @@ def per_query_summary(per_q):
 
 # ----------------------------------------------------------- measurement --
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    polled every 5 ms from a thread (the timed steps take tens of ms, too short
+    for nvidia-smi's sampling loop); the device is found by its PCI bus id, so
+    the index a process sees under CUDA_VISIBLE_DEVICES does not matter.
+    nvidia-smi at 200 ms is the fallback."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -180,8 +184,24 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.samples = []
+        self.h = None
+        self.stop_flag = False
 
     def start(self):
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.h = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -191,11 +211,34 @@ class ClockSampler:
         except FileNotFoundError:
             self.proc = None
 
+    def _poll(self):
+        nv = self.nv
+        mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        while not self.stop_flag:
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM), mx,
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+            except Exception:
+                break
+            time.sleep(0.005)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        if self.h is not None:
+            self.stop_flag = True
+            self.t.join(timeout=5)
+            nv = self.nv
+            bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            reasons = {n for _, _, r in self.samples for n, b in zip(names, bits) if r & b}
+            sm = [c for c, _, _ in self.samples]
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": self.samples[0][1] if self.samples else None,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "NVML, 5 ms"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -204,7 +247,6 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
@@ -218,7 +260,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def reduce_over_ranks(dev_ms, instances, dist, device):
