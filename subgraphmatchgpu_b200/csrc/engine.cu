@@ -200,42 +200,6 @@ __global__ void k_split(const uint64_t* __restrict__ incl, const uint64_t* __res
   }
 }
 
-// ---- pivot length of a step, sampled ---------------------------------------
-// The clipped pivot length of up to `ns` paths spread over the frontier (the
-// smallest list cut by the step's < and > conditions, as k_compute computes
-// it); the sum goes to acc[0].  The launch chooses between the warp per path
-// and the flattened kernel by the mean.
-__global__ void k_pivot_sample(DFront F, DStep s, DGraph G, uint32_t ns, unsigned long long* acc) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ns) return;
-  const uint32_t p = (uint32_t)(((uint64_t)i * F.P) / ns);
-  const uint32_t* piv = nullptr;
-  uint32_t n = 0xffffffffu;
-  for (int k = 0; k < s.nconn; ++k) {
-    const uint32_t* lp;
-    uint32_t ln;
-    AdjList(G, F.inst[s.conn[k]][p], lp, ln);
-    if (ln < n) {
-      n = ln;
-      piv = lp;
-    }
-  }
-  if (s.reuse >= 0) {
-    const uint32_t* lp;
-    uint32_t ln;
-    GetSet(F, s.reuse, p, lp, ln);
-    if (ln < n) {
-      n = ln;
-      piv = lp;
-    }
-  }
-  if (!piv) return;
-  const BoundsT<MAXV> bd = MakeBounds<MAXV>(s.cond, F, p);
-  uint32_t r0, r1;
-  Range(piv, n, bd, r0, r1);
-  if (r1 > r0) atomicAdd(acc, (unsigned long long)(r1 - r0));
-}
-
 // ---- paths grouped by the hub they probe ------------------------------------
 // A count step's membership tests land on the dense bitmap of the hub whose
 // list is searched.  Taken in frontier order, consecutive paths probe
@@ -1506,7 +1470,6 @@ class Executor {
   uint64_t cap_;
   int sms_ = 148;
   unsigned long long* ctrl_ = nullptr;  // [0] count [1] bytes [2] emitted [3] error flags [5] reuse hits
-                                        // [6] pivot sample
   uint64_t launches_ = 0, batches_ = 0, paths_ = 0, hot_ = 0, root_h2d_ = 0;
   const uint32_t* ext_cols_ = nullptr;
   uint64_t ext_bytes_ = 0;
@@ -1595,19 +1558,6 @@ class Executor {
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)sms_ * 16));
   }
   unsigned WarpGrid(uint64_t paths) const { return Grid(paths * 32, WARP_BLOCK); }
-
-  // Mean clipped pivot length of up to 4096 paths of the step (one small
-  // kernel and one read-back); infinite when the frontier is too small to
-  // matter.
-  double MeanPivot(const DFront& F, const DStep& ds, const DGraph& G) {
-    if (F.P < 4096) return 1e30;
-    const uint32_t ns = 4096;
-    unsigned long long* acc = ctrl_ + 6;
-    CK(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), st_));
-    k_pivot_sample<<<ns / 256, 256, 0, st_>>>(F, ds, G, ns, acc);
-    Launched();
-    return (double)ReadU64(reinterpret_cast<const uint64_t*>(acc)) / ns;
-  }
 
   // The order in which a count step takes its paths: grouped by the hub
   // slot of the step's last list vertex (the most recently materialised one,
@@ -1716,15 +1666,6 @@ class Executor {
       else
         k_compute<MODE, 4, MAXV, 0, false, true><<<WarpGrid(F.P), WARP_BLOCK, 0, st_>>>(
             F, ds, G, est, b0, ptr, cnt, data, cap, acc, err, DHeavy{});
-    } else if (gran == 0 && flat_below_ > 0 && nlists >= 2 && ds.msrc < 0 && MeanPivot(F, ds, G) < flat_below_) {
-      // auto: short clipped pivots leave most lanes of a warp per path idle;
-      // the flattened kernel packs 32 paths per warp
-      if (nlists <= 2)
-        LaunchFlat<MODE, 8, 2>(has_ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
-      else if (nlists <= 3)
-        LaunchFlat<MODE, 6, 3>(has_ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
-      else
-        LaunchFlat<MODE, 4, MAXV>(has_ne, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
     } else if (gran == 4 && nlists == 2 && !has_ne) {
       // warp per path; paths with a long clipped pivot go to a CTA each
       const size_t mark = A_.Mark();
@@ -1780,7 +1721,6 @@ class Executor {
   int gran_ = 0;
   uint32_t heavy_min_ = 2048;  // granularity 4: shortest pivot that gets a CTA
   bool group_by_hub_ = false;  // count steps take their paths hub by hub
-  double flat_below_ = 0;      // auto: flattened kernel when the mean pivot is shorter
   bool use_bitmaps_ = true;
 
  private:
@@ -2080,7 +2020,6 @@ RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& c
   ex.use_bitmaps_ = !(tuning & 0x100);
   if (const char* e = std::getenv("SME_HEAVY_PIVOT")) ex.heavy_min_ = (uint32_t)std::max(32L, std::atol(e));
   if (const char* e = std::getenv("SME_GROUP_BY_HUB")) ex.group_by_hub_ = std::atoi(e) != 0;
-  if (const char* e = std::getenv("SME_FLAT_BELOW")) ex.flat_below_ = std::atof(e);
   return ex.Run(t);
 }
 
