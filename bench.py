@@ -211,13 +211,19 @@ class ClockSampler:
         except FileNotFoundError:
             self.proc = None
 
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
+
     def _poll(self):
         nv = self.nv
         mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
         while not self.stop_flag:
             try:
                 self.samples.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM), mx,
-                                     nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(self.h), time.perf_counter()))
             except Exception:
                 break
             time.sleep(0.005)
@@ -234,11 +240,15 @@ class ClockSampler:
             nv = self.nv
             bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
                     nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
-            reasons = {n for _, _, r in self.samples for n, b in zip(names, bits) if r & b}
-            sm = [c for c, _, _ in self.samples]
+            t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
+            timed = [x for x in self.samples if t0 <= x[3] <= t1]
+            use, window = (timed, "timed steps") if len(timed) >= 3 else (self.samples, "warm-up and timed steps")
+            reasons = {n for _, _, r, _ in use for n, b in zip(names, bits) if r & b}
+            sm = [c for c, _, _, _ in use]
             return {"sm_mhz": statistics.median(sm) if sm else None,
                     "sm_max_mhz": self.samples[0][1] if self.samples else None,
-                    "reasons": sorted(reasons), "samples": len(sm), "source": "NVML, 5 ms"}
+                    "reasons": sorted(reasons), "samples": len(sm), "timed_samples": len(timed),
+                    "window": window, "source": "NVML, 5 ms"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -788,14 +798,17 @@ def main():
         c = gr.count(q, args.algo, roots=roots, device=local, **tune)
         return c, sme.last_stats()
 
+    # the sampler runs from the warm-up on; the timed window's own samples are
+    # reported when there are enough of them (the timed steps take tens of ms)
+    clocks = ClockSampler(local)
+    clocks.start()
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
     torch.cuda.synchronize()
+    clocks.mark_start()
     total_inst, dev_ms, kern_ms, alg_bytes, hot, launches = 0, 0.0, 0.0, 0, 0, 0
     per_q, counts = {}, {}
     for i in range(args.warmup, args.warmup + args.steps):
@@ -812,6 +825,7 @@ def main():
         e[1] += s.device_ms / 1e3
         e[2] += 1
     torch.cuda.synchronize()
+    clocks.mark_end()
     clk = clocks.stop()
     dev_ms_max, inst_all = reduce_over_ranks(dev_ms, total_inst, dist, "cuda")
     value = inst_all / (dev_ms_max / 1e3)
