@@ -81,6 +81,9 @@ def parse(argv=None):
     ap.add_argument("--no-s22", action="store_true", help="skip the R-MAT s22 legs")
     ap.add_argument("--no-l2-flush", action="store_true", help="do not flush L2 between steps")
     ap.add_argument("--threads", type=int, default=0, help="CPU threads (0: all)")
+    ap.add_argument("--profile-house", type=int, default=0,
+                    help="N: only count the house (LIGHT) on the bench graph over the first N roots of degree "
+                         "<= hub_degree in a seeded order once (a small case for a profiler capture) and exit")
     ap.add_argument("--profile-s22", default="",
                     help="BEGIN:END:STRIDE: only count the 4-clique of the degree-oriented R-MAT s22 graph over "
                          "roots BEGIN, BEGIN+STRIDE, ... < END once (a small case for a profiler capture), print "
@@ -738,6 +741,24 @@ def bench_s22(args, device, tune, peak):
     return out
 
 
+def profile_house(args):
+    """One count of the house (LIGHT plan) on the bench's R-MAT graph over a
+    block of non-hub roots (the plan roots the house at u1), resident: the
+    house's kernels for a profiler capture."""
+    import subgraphmatchgpu_b200 as sme
+    g = engine_graph(args)
+    rp, _ = g.csr()
+    deg = np.diff(rp).astype(np.int64)
+    roots = np.random.default_rng(args.seed * 1000 + 4).permutation(np.flatnonzero(deg <= args.hub_degree))
+    roots = roots[:args.profile_house].astype(np.uint32)
+    g.to_device(0)
+    c = g.count(4, sme.GPU_LIGHT, roots=roots, warp_granularity=args.granularity)
+    s = sme.last_stats()
+    print(json.dumps({"roots": len(roots), "instances": c, "device_ms": s.device_ms, "kernel_ms": s.kernel_ms,
+                      "algorithmic_bytes": s.algorithmic_bytes, "launches": s.kernel_launches,
+                      "hot_launches": s.hot_launches, "phase_ms": list(s.phase_ms)}), flush=True)
+
+
 def profile_s22(args):
     """One count of the 4-clique over a root range of the degree-oriented
     R-MAT s22 ef16 graph (the graph of the s22 legs), resident, with the
@@ -765,6 +786,8 @@ def main():
         return run_reference(args, rank, world)
     if args.profile_s22:
         return profile_s22(args)
+    if args.profile_house:
+        return profile_house(args)
 
     import torch
     import subgraphmatchgpu_b200 as sme
