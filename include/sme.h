@@ -198,6 +198,25 @@ int32_t sme_graph_is_oriented(const sme_graph* g);
  * on that device reuse it (inputs resident in HBM). */
 sme_status sme_graph_to_device(sme_graph* g, int device);
 sme_status sme_graph_release_device(sme_graph* g);
+/* Device addresses of the resident copy on `device` (after
+ * sme_graph_to_device): uint64 row_ptrs[n+1] and uint32 cols[m], valid until
+ * the copy is released; for sme_count_noalloc and the caller's own kernels.
+ * SME_ERR_INVALID_ARG when the graph is not resident there.  The reference
+ * keeps the same arrays in its GPU CSR (CSRGraph's device row_ptrs/cols). */
+sme_status sme_graph_device_arrays(const sme_graph* g, int device, const uint64_t** row_ptrs,
+                                   const uint32_t** cols);
+/* Keeps a packed copy of the adjacency lists in pinned host memory; every
+ * later upload of this graph (sme_graph_to_device, or a call on a graph that
+ * is not resident) copies the packed lists and expands them on the device
+ * into the same CSR.  Each list is stored as deltas from the previous element
+ * in blocks of 32 with one bit width per block (about 0.4x the bytes of the
+ * uint32 lists on R-MAT graphs), so the host->device copy shrinks by that
+ * much.  The packed copy reflects the lists when this is called: a borrowed
+ * CSR (sme_graph_from_csr, copy = 0) changed afterwards must be packed again.
+ * enable = 0 drops it.  *packed_bytes (may be NULL) receives the bytes an
+ * upload now copies.  No counterpart in the reference, which copies the
+ * uint32 CSR. */
+sme_status sme_graph_pack(sme_graph* g, int enable, uint64_t* packed_bytes);
 sme_status sme_graph_free(sme_graph* g);
 
 /* ---- seeded synthetic graphs (all passed through the preprocess step) ---- */

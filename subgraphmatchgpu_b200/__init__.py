@@ -112,6 +112,8 @@ SIGNATURES = {
     "sme_graph_is_oriented": (C.c_int32, [_P]),
     "sme_graph_to_device": (C.c_int, [_P, C.c_int]),
     "sme_graph_release_device": (C.c_int, [_P]),
+    "sme_graph_device_arrays": (C.c_int, [_P, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "sme_graph_pack": (C.c_int, [_P, C.c_int, C.POINTER(C.c_uint64)]),
     "sme_graph_free": (C.c_int, [_P]),
     "sme_generate_rmat": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, _U64, _PP]),
     "sme_generate_er": (C.c_int, [_U64, C.c_double, _U64, _PP]),
@@ -326,6 +328,20 @@ class Graph:
 
     def release_device(self) -> None:
         _check(lib().sme_graph_release_device(self._h))
+
+    def device_arrays(self, device: int = 0):
+        """Device addresses (row_ptrs, cols) of the resident copy on `device`."""
+        rp, cl = C.c_void_p(), C.c_void_p()
+        _check(lib().sme_graph_device_arrays(self._h, device, C.byref(rp), C.byref(cl)))
+        return rp.value, cl.value
+
+    def pack(self, enable: bool = True) -> int:
+        """Keeps a packed copy of the lists in pinned host memory; uploads copy
+        it and expand it on the device.  Returns the bytes an upload copies
+        (0 after pack(False))."""
+        b = C.c_uint64()
+        _check(lib().sme_graph_pack(self._h, int(bool(enable)), C.byref(b)))
+        return b.value
 
     def count(self, query: int, algo: int = GPU_LIGHT, mode: int = IN_MEMORY_GPU, **kw) -> int:
         o = opts(query, algo, mode, **kw)

@@ -321,6 +321,28 @@ sme_status sme_graph_to_device(sme_graph* g, int device) {
   });
 }
 
+sme_status sme_graph_device_arrays(const sme_graph* g, int device, const uint64_t** row_ptrs,
+                                   const uint32_t** cols) {
+  if (!g) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    const DeviceGraph* d = g->g.dev;
+    if (!d || d->device != device) Fail(SME_ERR_INVALID_ARG, "the graph is not resident on that device");
+    if (row_ptrs) *row_ptrs = d->row_ptrs;
+    if (cols) *cols = d->cols;
+  });
+}
+
+sme_status sme_graph_pack(sme_graph* g, int enable, uint64_t* packed_bytes) {
+  if (!g) return SME_ERR_INVALID_ARG;
+  return Guard([&] {
+    if (enable)
+      g->g.packed = PackLists(g->g);
+    else
+      g->g.packed.reset();
+    if (packed_bytes) *packed_bytes = g->g.packed ? g->g.packed->total : 0;
+  });
+}
+
 sme_status sme_graph_release_device(sme_graph* g) {
   if (!g) return SME_ERR_INVALID_ARG;
   return Guard([&] {

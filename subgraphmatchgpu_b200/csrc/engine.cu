@@ -1214,6 +1214,32 @@ __global__ void k_build_bitmaps(const uintE* __restrict__ rp, const uint32_t* __
   }
 }
 
+// One hub's bitmap per CTA, built in shared memory and written out whole (no
+// memset of the bitmaps and no global atomics); for bitmaps of up to
+// kSmemBitmapBytes.
+constexpr uint32_t kSmemBitmapBytes = 200u << 10;
+__global__ void __launch_bounds__(1024) k_build_bitmaps_smem(const uintE* __restrict__ rp,
+                                                             const uint32_t* __restrict__ cols,
+                                                             const uint32_t* __restrict__ hubs, uint32_t words,
+                                                             uint32_t* bm) {
+  extern __shared__ uint32_t row_s[];
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) row_s[i] = 0;
+  __syncthreads();
+  const uint32_t v = hubs[blockIdx.x];
+  for (uintE j = rp[v] + threadIdx.x; j < rp[v + 1]; j += blockDim.x) {
+    const uint32_t w = cols[j];
+    atomicOr(row_s + (w >> 5), 1u << (w & 31));
+  }
+  __syncthreads();
+  uint32_t* row = bm + (size_t)blockIdx.x * words;
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) row[i] = row_s[i];
+}
+
+__global__ void k_set_slots(const uint32_t* __restrict__ hubs, uint32_t nh, int32_t* slot) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += gridDim.x * blockDim.x)
+    slot[hubs[i]] = (int32_t)i;
+}
+
 // Bitmaps for the vertices of highest degree (>= kHubMinDegree) within a
 // byte budget (SME_HUB_BITMAP_MB, default 1 GiB, at most a quarter of the
 // device memory `room` the caller can spare); a bitmap is n bits.  Measured
@@ -1221,45 +1247,186 @@ __global__ void k_build_bitmaps(const uintE* __restrict__ rp, const uint32_t* __
 // 1 GiB 10.5e9, 2 GiB 10.7e9 instances/s, flat beyond; whole-graph counts
 // flat from 512 MiB.  `alloc` hands out device memory (cudaMalloc, or the
 // context's arena for a per-call upload); `scratch_owned` frees the
-// temporary hub list afterwards.
+// temporary hub list afterwards.  The hub choice is cached on the host graph;
+// the slot array is filled on the device.  Returns the host->device bytes.
 template <typename Alloc>
-void BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream, Alloc alloc, bool scratch_owned,
-                     uint64_t room) {
+uint64_t BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream, Alloc alloc, bool scratch_owned,
+                         uint64_t room) {
   uint64_t kHubMinDegree = 256;
   if (const char* e = std::getenv("SME_HUB_MIN_DEGREE")) kHubMinDegree = std::strtoull(e, nullptr, 10);
   uint64_t budget = 1024ULL << 20;
   if (const char* e = std::getenv("SME_HUB_BITMAP_MB")) budget = std::strtoull(e, nullptr, 10) << 20;
   budget = std::min<uint64_t>(budget, room / 4);
   const uint32_t words = (uint32_t)((g.n + 31) / 32);
-  if (budget == 0 || words == 0) return;
+  if (budget == 0 || words == 0) return 0;
   const uint64_t max_hubs = budget / ((uint64_t)words * 4);
-  std::vector<std::pair<uint64_t, uint32_t>> cand;
-  for (uint64_t u = 0; u < g.n; ++u) {
-    uint64_t deg = g.row_ptrs[u + 1] - g.row_ptrs[u];
-    if (deg >= kHubMinDegree) cand.emplace_back(deg, (uint32_t)u);
-  }
-  if (cand.empty() || max_hubs == 0) return;
-  std::sort(cand.begin(), cand.end(), [](const std::pair<uint64_t, uint32_t>& a,
-                                         const std::pair<uint64_t, uint32_t>& b) { return a.first > b.first; });
-  if (cand.size() > max_hubs) cand.resize(max_hubs);
-  std::vector<int32_t> slot(g.n, -1);
-  std::vector<uint32_t> hubs(cand.size());
-  for (size_t i = 0; i < cand.size(); ++i) {
-    hubs[i] = cand[i].second;
-    slot[cand[i].second] = (int32_t)i;
-  }
+  if (max_hubs == 0) return 0;
+  std::shared_ptr<const std::vector<uint32_t>> order = g.HubOrder(kHubMinDegree);
+  if (order->empty()) return 0;
+  std::vector<uint32_t> hubs(order->begin(), order->begin() + std::min<uint64_t>(order->size(), max_hubs));
+  std::sort(hubs.begin(), hubs.end());  // slots in id order
+  const uint32_t nh = (uint32_t)hubs.size();
   d->hub_slot = (int32_t*)alloc(g.n * sizeof(int32_t));
-  d->bitmaps = (uint32_t*)alloc(hubs.size() * (size_t)words * 4);
-  uint32_t* d_hubs = (uint32_t*)alloc(hubs.size() * 4);
-  CK(cudaMemcpyAsync(d->hub_slot, slot.data(), g.n * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
-  CK(cudaMemcpyAsync(d_hubs, hubs.data(), hubs.size() * 4, cudaMemcpyHostToDevice, stream));
-  CK(cudaMemsetAsync(d->bitmaps, 0, hubs.size() * (size_t)words * 4, stream));
-  k_build_bitmaps<<<(unsigned)hubs.size(), 256, 0, stream>>>(d->row_ptrs, d->cols, d_hubs, words, d->bitmaps);
+  d->bitmaps = (uint32_t*)alloc((size_t)nh * words * 4);
+  uint32_t* d_hubs = (uint32_t*)alloc((size_t)nh * 4);
+  CK(cudaMemcpyAsync(d_hubs, hubs.data(), (size_t)nh * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemsetAsync(d->hub_slot, 0xFF, g.n * sizeof(int32_t), stream));
+  k_set_slots<<<std::min<uint32_t>((nh + 255) / 256, 1184), 256, 0, stream>>>(d_hubs, nh, d->hub_slot);
+  if ((uint64_t)words * 4 <= kSmemBitmapBytes) {
+    CK(cudaFuncSetAttribute(k_build_bitmaps_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)kSmemBitmapBytes));
+    k_build_bitmaps_smem<<<nh, 1024, (size_t)words * 4, stream>>>(d->row_ptrs, d->cols, d_hubs, words,
+                                                                   d->bitmaps);
+  } else {
+    CK(cudaMemsetAsync(d->bitmaps, 0, (size_t)nh * words * 4, stream));
+    k_build_bitmaps<<<nh, 256, 0, stream>>>(d->row_ptrs, d->cols, d_hubs, words, d->bitmaps);
+  }
   CK(cudaStreamSynchronize(stream));
   CK(cudaGetLastError());
   if (scratch_owned) cudaFree(d_hubs);
   d->words = words;
-  d->nhubs = (uint32_t)hubs.size();
+  d->nhubs = nh;
+  return (uint64_t)nh * 4;
+}
+
+// ------------------------------------------------------------ packed lists --
+// rp[0] = 0, rp[i + 1] = deg[i] (then an inclusive scan of rp + 1).
+__global__ void k_deg_to_rp(const uint32_t* __restrict__ deg, uint64_t n, uintE* rp) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += (uint64_t)gridDim.x * blockDim.x)
+    rp[i] = i ? deg[i - 1] : 0;
+}
+
+// Expands the packed lists (format: PackedLists, sme_internal.h) into cols.
+// One warp per (list, segment): warps [0, n) take segment 0 of list w, warps
+// [n, n + nsegs) the segments named in segs.  The warp reads the segment's
+// block widths (one per lane), scans the blocks' byte sizes to place every
+// block, then per block extracts one delta per lane and adds the running
+// value through a warp scan.  Every offset read from the buffer is checked
+// against the stream before use: a bad one sets *flag and skips the segment.
+__global__ void __launch_bounds__(256) k_unpack_lists(const uint32_t* __restrict__ deg,
+                                                      const uint32_t* __restrict__ woff,
+                                                      const uint64_t* __restrict__ segs, uint64_t n, uint64_t nsegs,
+                                                      const uint32_t* __restrict__ stream, uint64_t stream_words,
+                                                      const uintE* __restrict__ rp, uint64_t m, uintV* cols,
+                                                      uint32_t* flag) {
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (w >= n + nsegs) return;  // uniform in the warp
+  uint64_t v;
+  uint32_t s;
+  if (w < n) {
+    v = w;
+    s = 0;
+  } else {
+    const uint64_t e = segs[w - n];
+    v = e >> 32;
+    s = (uint32_t)e;
+  }
+  if (v >= n) {
+    if (lane == 0) atomicOr(flag, 1u);
+    return;
+  }
+  const uint64_t d = deg[v];
+  const uint64_t nseg = (d + kPackSegment - 1) / kPackSegment;
+  if (s >= nseg) {
+    if (s > 0 && lane == 0) atomicOr(flag, 1u);
+    return;
+  }
+  const uint64_t stream_bytes = stream_words * 4;
+  const uint64_t list = (uint64_t)woff[v] * 4;
+  uint32_t base = 0;
+  uint64_t seg = list + 8 * (nseg - 1);
+  if (s > 0) {
+    const uint64_t ti = (list >> 2) + 2 * (uint64_t)(s - 1);
+    if (ti + 1 >= stream_words) {
+      if (lane == 0) atomicOr(flag, 1u);
+      return;
+    }
+    base = stream[ti];
+    seg = list + stream[ti + 1];
+  }
+  const uint64_t e0 = (uint64_t)s * kPackSegment;
+  const uint32_t ne = (uint32_t)(d - e0 < kPackSegment ? d - e0 : kPackSegment);
+  const uint32_t nb = (ne + 31) / 32;
+  const uint64_t out0 = rp[v] + e0;
+  if (seg + nb + 8 > stream_bytes || out0 + ne > m) {
+    if (lane == 0) atomicOr(flag, 1u);
+    return;
+  }
+  const uint8_t* bytes = reinterpret_cast<const uint8_t*>(stream);
+  const uint32_t width = lane < nb ? bytes[seg + lane] : 0;
+  const uint32_t cnt = lane < nb ? min(32u, ne - 32 * lane) : 0;
+  const uint32_t sz = (cnt * width + 7) / 8;
+  uint32_t incl = sz;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(FULL, incl, 31);
+  if (__any_sync(FULL, width > 32) || seg + nb + total + 8 > stream_bytes) {
+    if (lane == 0) atomicOr(flag, 1u);
+    return;
+  }
+  const uint64_t off = seg + nb + (incl - sz);  // byte start of this lane's block
+  uintV* out = cols + out0;
+  uint32_t prev = base;
+  for (uint32_t t = 0; t < nb; ++t) {
+    const uint32_t b = __shfl_sync(FULL, width, t);
+    const uint32_t c = __shfl_sync(FULL, cnt, t);
+    const uint64_t o = __shfl_sync(FULL, (unsigned long long)off, t);
+    uint32_t delta = 0;
+    if (lane < c && b) {
+      const uint64_t bit = o * 8 + (uint64_t)lane * b;
+      const uint64_t wi = bit >> 5;
+      delta = __funnelshift_r(stream[wi], stream[wi + 1], (uint32_t)bit & 31);
+      if (b < 32) delta &= (1u << b) - 1u;
+    }
+#pragma unroll
+    for (int o2 = 1; o2 < 32; o2 <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, delta, o2);
+      if (lane >= o2) delta += y;
+    }
+    const uint32_t val = prev + delta;
+    if (lane < c) out[32 * t + lane] = val;
+    prev = __shfl_sync(FULL, val, 31);
+  }
+}
+
+uint32_t ScanBlocks(uint64_t n) { return (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE); }
+
+// Copies the packed lists into `scratch` (device, pk.total bytes) and expands
+// them into rp (n + 1) and cols (m) on `st`.  `bs` holds ScanBlocks(n) words,
+// `flag` one word (set by a bad offset).
+void UnpackLists(const PackedLists& pk, uint8_t* scratch, uint64_t* bs, uint32_t* flag, uintE* rp, uintV* cols,
+                 cudaStream_t st) {
+  const uint64_t n = pk.n;
+  CK(cudaMemcpyAsync(scratch, pk.base, pk.total, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(flag, 0, sizeof(uint32_t), st));
+  const uint32_t* deg = reinterpret_cast<const uint32_t*>(scratch + pk.deg_at);
+  k_deg_to_rp<<<(unsigned)std::min<uint64_t>((n + 256) / 256, 148 * 8), 256, 0, st>>>(deg, n, rp);
+  if (n) {
+    const uint32_t nb = ScanBlocks(n);
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, st>>>(rp + 1, (uint32_t)n, bs);
+    k_scan_partials<<<1, 1024, 0, st>>>(bs, nb);
+    k_scan_apply<<<nb, SCAN_THREADS, 0, st>>>(rp + 1, (uint32_t)n, bs);
+  }
+  const uint64_t items = n + pk.nsegs;
+  if (items)
+    k_unpack_lists<<<(unsigned)((items * 32 + 255) / 256), 256, 0, st>>>(
+        deg, reinterpret_cast<const uint32_t*>(scratch + pk.woff_at),
+        reinterpret_cast<const uint64_t*>(scratch + pk.segs_at), n, pk.nsegs,
+        reinterpret_cast<const uint32_t*>(scratch + pk.stream_at), pk.stream_bytes / 4, rp, pk.m, cols, flag);
+  CK(cudaGetLastError());
+}
+
+void CheckPacked(const HostGraph& g, const PackedLists& pk) {
+  if (pk.n != g.n || pk.m != g.m) Fail(SME_ERR_INVALID_ARG, "packed lists do not match the graph");
+  if (pk.n > UINT32_MAX) Fail(SME_ERR_INVALID_ARG, "packed upload needs n < 2^32");
+}
+
+void FailOnFlag(uint32_t flag) {
+  if (flag) Fail(SME_ERR_CUDA, "packed lists are corrupt: an offset points outside the stream");
 }
 }  // namespace
 
@@ -1269,25 +1436,45 @@ DeviceGraph* UploadGraph(const HostGraph& g, int device, cudaStream_t stream, ui
   d->device = device;
   d->n = g.n;
   d->m = g.m;
+  uint64_t bytes = 0;
+  std::shared_ptr<const PackedLists> pk = g.packed;
+  uint8_t* scratch = nullptr;
   try {
     CK(cudaMalloc((void**)&d->row_ptrs, (g.n + 1) * sizeof(uintE)));
     CK(cudaMalloc((void**)&d->cols, std::max<uint64_t>(g.m, 1) * sizeof(uintV)));
-    CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, stream));
-    if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, stream));
-    CK(cudaStreamSynchronize(stream));
-    auto dev_alloc = [](size_t bytes) {
+    if (pk) {
+      CheckPacked(g, *pk);
+      const uint64_t bs_at = (pk->total + 15) & ~uint64_t(15);
+      CK(cudaMalloc((void**)&scratch, bs_at + (uint64_t)ScanBlocks(g.n) * 8 + 16));
+      uint32_t* flag = reinterpret_cast<uint32_t*>(scratch + bs_at + (uint64_t)ScanBlocks(g.n) * 8);
+      UnpackLists(*pk, scratch, reinterpret_cast<uint64_t*>(scratch + bs_at), flag, d->row_ptrs, d->cols, stream);
+      uint32_t h_flag = 0;
+      CK(cudaMemcpyAsync(&h_flag, flag, 4, cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      cudaFree(scratch);
+      scratch = nullptr;
+      FailOnFlag(h_flag);
+      bytes = pk->total;
+    } else {
+      CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, stream));
+      if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, stream));
+      CK(cudaStreamSynchronize(stream));
+      bytes = (g.n + 1) * sizeof(uintE) + g.m * sizeof(uintV);
+    }
+    auto dev_alloc = [](size_t b) {
       void* p = nullptr;
-      CK(cudaMalloc(&p, bytes));
+      CK(cudaMalloc(&p, b));
       return p;
     };
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot));
-    BuildHubBitmaps(d, g, stream, dev_alloc, true, fr);
+    bytes += BuildHubBitmaps(d, g, stream, dev_alloc, true, fr);
   } catch (...) {
+    if (scratch) cudaFree(scratch);
     FreeDeviceGraph(d);
     throw;
   }
-  if (h2d) *h2d += (g.n + 1) * sizeof(uintE) + g.m * sizeof(uintV);
+  if (h2d) *h2d += bytes;
   return d;
 }
 
@@ -1298,19 +1485,41 @@ DeviceGraph* UploadGraphToArena(const HostGraph& g, DeviceContext& ctx, uint64_t
   d->n = g.n;
   d->m = g.m;
   d->in_arena = true;
+  uint64_t bytes = 0;
+  std::shared_ptr<const PackedLists> pk = g.packed;
   try {
-    auto arena_alloc = [&ctx](size_t bytes) { return ctx.arena.Alloc(bytes); };
+    auto arena_alloc = [&ctx](size_t b) { return ctx.arena.Alloc(b); };
     d->row_ptrs = (uintE*)arena_alloc((g.n + 1) * sizeof(uintE));
     d->cols = (uintV*)arena_alloc(std::max<uint64_t>(g.m, 1) * sizeof(uintV));
-    CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, ctx.stream));
-    if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, ctx.stream));
-    BuildHubBitmaps(d, g, ctx.stream, arena_alloc, false, ctx.arena.Free());
+    uint32_t* flag = nullptr;
+    if (pk) {
+      CheckPacked(g, *pk);
+      flag = (uint32_t*)arena_alloc(sizeof(uint32_t));
+      // the copy's scratch is released before the bitmaps take the same
+      // space: both are ordered on the context's stream
+      const size_t mark = ctx.arena.Mark();
+      uint8_t* scratch = (uint8_t*)arena_alloc(pk->total);
+      uint64_t* bs = (uint64_t*)arena_alloc((size_t)ScanBlocks(g.n) * 8);
+      UnpackLists(*pk, scratch, bs, flag, d->row_ptrs, d->cols, ctx.stream);
+      ctx.arena.Release(mark);
+      bytes = pk->total;
+    } else {
+      CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, ctx.stream));
+      if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, ctx.stream));
+      bytes = (g.n + 1) * sizeof(uintE) + g.m * sizeof(uintV);
+    }
+    bytes += BuildHubBitmaps(d, g, ctx.stream, arena_alloc, false, ctx.arena.Free());
+    if (flag) {
+      CK(cudaMemcpyAsync(ctx.h_pinned, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx.stream));
+      CK(cudaStreamSynchronize(ctx.stream));
+      FailOnFlag(*reinterpret_cast<const uint32_t*>(ctx.h_pinned));
+    }
     CK(cudaStreamSynchronize(ctx.stream));
   } catch (...) {
     delete d;
     throw;
   }
-  if (h2d) *h2d += (g.n + 1) * sizeof(uintE) + g.m * sizeof(uintV);
+  if (h2d) *h2d += bytes;
   return d;
 }
 

@@ -45,8 +45,32 @@ bool HostGraph::LoopFree() const {
   return f == 1;
 }
 
+std::shared_ptr<const std::vector<uint32_t>> HostGraph::HubOrder(uint64_t min_degree) const {
+  std::lock_guard<std::mutex> lock(hub_mu_);
+  if (hub_order_ && hub_order_min_ == min_degree) return hub_order_;
+  std::vector<std::pair<uint64_t, uint32_t>> cand;
+  for (uint64_t u = 0; u < n; ++u) {
+    uint64_t deg = row_ptrs[u + 1] - row_ptrs[u];
+    if (deg >= min_degree) cand.emplace_back(deg, (uint32_t)u);
+  }
+  std::sort(cand.begin(), cand.end(), [](const std::pair<uint64_t, uint32_t>& a,
+                                         const std::pair<uint64_t, uint32_t>& b) {
+    return a.first != b.first ? a.first > b.first : a.second < b.second;
+  });
+  auto order = std::make_shared<std::vector<uint32_t>>(cand.size());
+  for (size_t i = 0; i < cand.size(); ++i) (*order)[i] = cand[i].second;
+  hub_order_ = order;
+  hub_order_min_ = min_degree;
+  return hub_order_;
+}
+
 void HostGraph::Adopt(std::vector<uintE>&& r, std::vector<uintV>&& c) {
   loop_free.store(-1, std::memory_order_relaxed);
+  packed.reset();
+  {
+    std::lock_guard<std::mutex> lock(hub_mu_);
+    hub_order_.reset();
+  }
   row_store = std::move(r);
   col_store = std::move(c);
   n = row_store.empty() ? 0 : row_store.size() - 1;

@@ -6,6 +6,8 @@
 #include <atomic>
 #include <cstdint>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -31,6 +33,37 @@ struct Error : public std::runtime_error {
 void SetLastError(const std::string& msg);
 
 // ---------------------------------------------------------------- graphs --
+// Packed copy of a graph's adjacency lists in pinned host memory
+// (sme_graph_pack): what an upload of a non-resident graph copies over the
+// host link, expanded on the device by k_unpack_lists (engine.cu).
+//
+// One contiguous buffer:
+//   deg[n]    uint32 list lengths
+//   woff[n]   uint32 start of each list in `stream`, in 4-byte words
+//   segs[ns]  uint64 (vertex << 32 | segment) for every segment >= 1 of every
+//             list (8-byte aligned)
+//   stream    the lists, each on a 4-byte boundary, then 8 zero bytes
+// A list of d elements is cut into segments of kPackSegment elements.  A list
+// of S segments starts with S-1 table entries (uint32 value of the element
+// before the segment, uint32 byte offset of the segment from the list start),
+// then its segments.  A segment holds its blocks of 32 elements (the last one
+// shorter): one width byte per block, then each block's deltas at `width`
+// bits apiece, least significant bit first, every block on a byte boundary.
+// An element's delta is its difference from the element before it in the
+// list (from 0 for the first), modulo 2^32, so any list round-trips and
+// sorted lists pack small.
+constexpr uint32_t kPackSegment = 1024;
+struct PackedLists {
+  uint64_t n = 0, m = 0, nsegs = 0;
+  uint8_t* base = nullptr;  // the buffer
+  uint64_t total = 0;       // bytes of the buffer (what an upload copies)
+  uint64_t deg_at = 0, woff_at = 0, segs_at = 0, stream_at = 0, stream_bytes = 0;  // byte offsets / size
+  bool pinned = false;
+  ~PackedLists();
+};
+struct HostGraph;
+std::shared_ptr<const PackedLists> PackLists(const HostGraph& g);
+
 // Host CSR.  Owns its arrays unless `borrowed`.
 struct DeviceGraph;  // engine.cu
 struct HostGraph {
@@ -46,8 +79,18 @@ struct HostGraph {
   std::vector<uintE> row_store;
   std::vector<uintV> col_store;
   DeviceGraph* dev = nullptr;  // resident device copy (may be null)
+  // packed lists an upload copies instead of the CSR (null = plain CSR)
+  std::shared_ptr<const PackedLists> packed;
   uint64_t MaxDegree() const;
   void Adopt(std::vector<uintE>&& r, std::vector<uintV>&& c);
+  // Vertices of degree >= min_degree, highest degree first (ties by id);
+  // computed once per graph and threshold and shared by every upload.
+  std::shared_ptr<const std::vector<uint32_t>> HubOrder(uint64_t min_degree) const;
+
+ private:
+  mutable std::mutex hub_mu_;
+  mutable std::shared_ptr<const std::vector<uint32_t>> hub_order_;
+  mutable uint64_t hub_order_min_ = 0;
 };
 
 void ReadBinFile(const std::string& path, HostGraph& g);

@@ -340,3 +340,15 @@ def test_lvid_names_are_exact_strings(tmp_path):
     with pytest.raises(sme.SmeError) as e:
         sme.Graph.load(str(f), 0)
     assert e.value.status == 2
+
+
+def test_pack_reports_the_bytes_an_upload_copies():
+    g = sme.Graph.rmat(12, 8, seed=3)
+    plain = (g.n + 1) * 8 + g.m * 4
+    b = g.pack()
+    assert 0 < b < 0.7 * plain
+    assert g.pack() == b  # deterministic
+    assert g.pack(False) == 0
+    with pytest.raises(sme.SmeError) as e:
+        g.device_arrays(0)
+    assert e.value.status == 1
