@@ -1178,6 +1178,8 @@ DeviceContext* CreateContext(int device, uint64_t bytes) {
   c->device = device;
   try {
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (auto& e : c->copy_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot));
     uint64_t want = bytes ? bytes : (uint64_t)(fr * 0.80);
@@ -1197,9 +1199,13 @@ void DestroyContext(DeviceContext* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   if (c->arena.base) cudaFree(c->arena.base);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  for (auto e : c->copy_ev)
+    if (e) cudaEventDestroy(e);
   delete c;
 }
 
@@ -1245,48 +1251,73 @@ __global__ void k_set_slots(const uint32_t* __restrict__ hubs, uint32_t nh, int3
 // device memory `room` the caller can spare); a bitmap is n bits.  Measured
 // on R-MAT s20 (root blocks of the bench): 256 MiB 9.5e9, 512 MiB 9.8e9,
 // 1 GiB 10.5e9, 2 GiB 10.7e9 instances/s, flat beyond; whole-graph counts
-// flat from 512 MiB.  `alloc` hands out device memory (cudaMalloc, or the
-// context's arena for a per-call upload); `scratch_owned` frees the
-// temporary hub list afterwards.  The hub choice is cached on the host graph;
-// the slot array is filled on the device.  Returns the host->device bytes.
+// flat from 512 MiB.  The hub choice is cached on the host graph; hubs take
+// slots in id order, so the hubs of a vertex range are a slot range.
+struct HubPlan {
+  std::shared_ptr<const std::vector<uint32_t>> sel;  // sorted ids; slot i holds (*sel)[i]
+  const std::vector<uint32_t>& hubs() const { return *sel; }
+  uint32_t* d_hubs = nullptr;
+  uint32_t words = 0;
+  bool smem = false;
+};
+
+// Chooses the hubs, allocates slot index + bitmaps + hub list with `alloc`,
+// and queues on `st` the hub-list copy, the slot fill and (global build only)
+// the clearing of the bitmaps.  False when no vertex gets a bitmap.
 template <typename Alloc>
-uint64_t BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream, Alloc alloc, bool scratch_owned,
-                         uint64_t room) {
+bool PlanHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t st, Alloc alloc, uint64_t room, HubPlan* hp) {
   uint64_t kHubMinDegree = 256;
   if (const char* e = std::getenv("SME_HUB_MIN_DEGREE")) kHubMinDegree = std::strtoull(e, nullptr, 10);
   uint64_t budget = 1024ULL << 20;
   if (const char* e = std::getenv("SME_HUB_BITMAP_MB")) budget = std::strtoull(e, nullptr, 10) << 20;
   budget = std::min<uint64_t>(budget, room / 4);
   const uint32_t words = (uint32_t)((g.n + 31) / 32);
-  if (budget == 0 || words == 0) return 0;
+  if (budget == 0 || words == 0) return false;
   const uint64_t max_hubs = budget / ((uint64_t)words * 4);
-  if (max_hubs == 0) return 0;
-  std::shared_ptr<const std::vector<uint32_t>> order = g.HubOrder(kHubMinDegree);
-  if (order->empty()) return 0;
-  std::vector<uint32_t> hubs(order->begin(), order->begin() + std::min<uint64_t>(order->size(), max_hubs));
-  std::sort(hubs.begin(), hubs.end());  // slots in id order
-  const uint32_t nh = (uint32_t)hubs.size();
+  if (max_hubs == 0) return false;
+  hp->sel = g.HubSelection(kHubMinDegree, max_hubs);
+  if (hp->sel->empty()) return false;
+  const uint32_t nh = (uint32_t)hp->sel->size();
+  hp->words = words;
+  hp->smem = (uint64_t)words * 4 <= kSmemBitmapBytes;
   d->hub_slot = (int32_t*)alloc(g.n * sizeof(int32_t));
   d->bitmaps = (uint32_t*)alloc((size_t)nh * words * 4);
-  uint32_t* d_hubs = (uint32_t*)alloc((size_t)nh * 4);
-  CK(cudaMemcpyAsync(d_hubs, hubs.data(), (size_t)nh * 4, cudaMemcpyHostToDevice, stream));
-  CK(cudaMemsetAsync(d->hub_slot, 0xFF, g.n * sizeof(int32_t), stream));
-  k_set_slots<<<std::min<uint32_t>((nh + 255) / 256, 1184), 256, 0, stream>>>(d_hubs, nh, d->hub_slot);
-  if ((uint64_t)words * 4 <= kSmemBitmapBytes) {
-    CK(cudaFuncSetAttribute(k_build_bitmaps_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)kSmemBitmapBytes));
-    k_build_bitmaps_smem<<<nh, 1024, (size_t)words * 4, stream>>>(d->row_ptrs, d->cols, d_hubs, words,
-                                                                   d->bitmaps);
-  } else {
-    CK(cudaMemsetAsync(d->bitmaps, 0, (size_t)nh * words * 4, stream));
-    k_build_bitmaps<<<nh, 256, 0, stream>>>(d->row_ptrs, d->cols, d_hubs, words, d->bitmaps);
-  }
-  CK(cudaStreamSynchronize(stream));
-  CK(cudaGetLastError());
-  if (scratch_owned) cudaFree(d_hubs);
+  hp->d_hubs = (uint32_t*)alloc((size_t)nh * 4);
+  CK(cudaMemcpyAsync(hp->d_hubs, hp->sel->data(), (size_t)nh * 4, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(d->hub_slot, 0xFF, g.n * sizeof(int32_t), st));
+  k_set_slots<<<std::min<uint32_t>((nh + 255) / 256, 1184), 256, 0, st>>>(hp->d_hubs, nh, d->hub_slot);
+  if (!hp->smem) CK(cudaMemsetAsync(d->bitmaps, 0, (size_t)nh * words * 4, st));
   d->words = words;
   d->nhubs = nh;
-  return (uint64_t)nh * 4;
+  return true;
+}
+
+// Builds the bitmaps of slots [first, first + count) from the device lists.
+void BuildHubRange(const DeviceGraph* d, const HubPlan& hp, uint32_t first, uint32_t count, cudaStream_t st) {
+  if (!count) return;
+  if (hp.smem) {
+    CK(cudaFuncSetAttribute(k_build_bitmaps_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)kSmemBitmapBytes));
+    k_build_bitmaps_smem<<<count, 1024, (size_t)hp.words * 4, st>>>(d->row_ptrs, d->cols, hp.d_hubs + first,
+                                                                     hp.words, d->bitmaps + (size_t)first * hp.words);
+  } else {
+    k_build_bitmaps<<<count, 256, 0, st>>>(d->row_ptrs, d->cols, hp.d_hubs + first, hp.words,
+                                           d->bitmaps + (size_t)first * hp.words);
+  }
+}
+
+// Plan + build of every hub, synchronised.  `scratch_owned` frees the hub
+// list afterwards (cudaMalloc'd).  Returns the host->device bytes.
+template <typename Alloc>
+uint64_t BuildHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t stream, Alloc alloc, bool scratch_owned,
+                         uint64_t room) {
+  HubPlan hp;
+  if (!PlanHubBitmaps(d, g, stream, alloc, room, &hp)) return 0;
+  BuildHubRange(d, hp, 0, (uint32_t)hp.hubs().size(), stream);
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaGetLastError());
+  if (scratch_owned) cudaFree(hp.d_hubs);
+  return (uint64_t)hp.hubs().size() * 4;
 }
 
 // ------------------------------------------------------------ packed lists --
@@ -1296,29 +1327,33 @@ __global__ void k_deg_to_rp(const uint32_t* __restrict__ deg, uint64_t n, uintE*
     rp[i] = i ? deg[i - 1] : 0;
 }
 
-// Expands the packed lists (format: PackedLists, sme_internal.h) into cols.
-// One warp per (list, segment): warps [0, n) take segment 0 of list w, warps
-// [n, n + nsegs) the segments named in segs.  The warp reads the segment's
-// block widths (one per lane), scans the blocks' byte sizes to place every
-// block, then per block extracts one delta per lane and adds the running
-// value through a warp scan.  Every offset read from the buffer is checked
-// against the stream before use: a bad one sets *flag and skips the segment.
+// Expands the packed lists (format: PackedLists, sme_internal.h) of lists
+// [v0, v1) into cols; their segments after the first are segs[s0, s1).
+// One warp per (list, segment): warps [0, v1 - v0) take segment 0 of list
+// v0 + w, the next s1 - s0 warps the segments named in segs.  The warp reads
+// the segment's block widths (one per lane), scans the blocks' byte sizes to
+// place every block, then per block extracts one delta per lane and adds the
+// running value through a warp scan.  Every offset read from the buffer is
+// checked against the stream before use: a bad one sets *flag and skips the
+// segment.
 __global__ void __launch_bounds__(256) k_unpack_lists(const uint32_t* __restrict__ deg,
                                                       const uint32_t* __restrict__ woff,
-                                                      const uint64_t* __restrict__ segs, uint64_t n, uint64_t nsegs,
+                                                      const uint64_t* __restrict__ segs, uint64_t n, uint64_t v0,
+                                                      uint64_t v1, uint64_t s0, uint64_t s1,
                                                       const uint32_t* __restrict__ stream, uint64_t stream_words,
                                                       const uintE* __restrict__ rp, uint64_t m, uintV* cols,
                                                       uint32_t* flag) {
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
-  if (w >= n + nsegs) return;  // uniform in the warp
+  const uint64_t nv = v1 - v0;
+  if (w >= nv + (s1 - s0)) return;  // uniform in the warp
   uint64_t v;
   uint32_t s;
-  if (w < n) {
-    v = w;
+  if (w < nv) {
+    v = v0 + w;
     s = 0;
   } else {
-    const uint64_t e = segs[w - n];
+    const uint64_t e = segs[s0 + (w - nv)];
     v = e >> 32;
     s = (uint32_t)e;
   }
@@ -1395,14 +1430,9 @@ __global__ void __launch_bounds__(256) k_unpack_lists(const uint32_t* __restrict
 
 uint32_t ScanBlocks(uint64_t n) { return (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE); }
 
-// Copies the packed lists into `scratch` (device, pk.total bytes) and expands
-// them into rp (n + 1) and cols (m) on `st`.  `bs` holds ScanBlocks(n) words,
-// `flag` one word (set by a bad offset).
-void UnpackLists(const PackedLists& pk, uint8_t* scratch, uint64_t* bs, uint32_t* flag, uintE* rp, uintV* cols,
-                 cudaStream_t st) {
+// row_ptrs from the packed degrees in `scratch` (copied there already).
+void PackedRowPtrs(const PackedLists& pk, const uint8_t* scratch, uint64_t* bs, uintE* rp, cudaStream_t st) {
   const uint64_t n = pk.n;
-  CK(cudaMemcpyAsync(scratch, pk.base, pk.total, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(flag, 0, sizeof(uint32_t), st));
   const uint32_t* deg = reinterpret_cast<const uint32_t*>(scratch + pk.deg_at);
   k_deg_to_rp<<<(unsigned)std::min<uint64_t>((n + 256) / 256, 148 * 8), 256, 0, st>>>(deg, n, rp);
   if (n) {
@@ -1411,12 +1441,28 @@ void UnpackLists(const PackedLists& pk, uint8_t* scratch, uint64_t* bs, uint32_t
     k_scan_partials<<<1, 1024, 0, st>>>(bs, nb);
     k_scan_apply<<<nb, SCAN_THREADS, 0, st>>>(rp + 1, (uint32_t)n, bs);
   }
-  const uint64_t items = n + pk.nsegs;
-  if (items)
-    k_unpack_lists<<<(unsigned)((items * 32 + 255) / 256), 256, 0, st>>>(
-        deg, reinterpret_cast<const uint32_t*>(scratch + pk.woff_at),
-        reinterpret_cast<const uint64_t*>(scratch + pk.segs_at), n, pk.nsegs,
-        reinterpret_cast<const uint32_t*>(scratch + pk.stream_at), pk.stream_bytes / 4, rp, pk.m, cols, flag);
+}
+
+// Expands lists [v0, v1) (segments segs[s0, s1)) from `scratch` into cols.
+void UnpackRange(const PackedLists& pk, const uint8_t* scratch, const uintE* rp, uintV* cols, uint32_t* flag,
+                 uint64_t v0, uint64_t v1, uint64_t s0, uint64_t s1, cudaStream_t st) {
+  const uint64_t items = (v1 - v0) + (s1 - s0);
+  if (!items) return;
+  k_unpack_lists<<<(unsigned)((items * 32 + 255) / 256), 256, 0, st>>>(
+      reinterpret_cast<const uint32_t*>(scratch + pk.deg_at), reinterpret_cast<const uint32_t*>(scratch + pk.woff_at),
+      reinterpret_cast<const uint64_t*>(scratch + pk.segs_at), pk.n, v0, v1, s0, s1,
+      reinterpret_cast<const uint32_t*>(scratch + pk.stream_at), pk.stream_bytes / 4, rp, pk.m, cols, flag);
+}
+
+// Copies the packed lists into `scratch` (device, pk.total bytes) and expands
+// them into rp (n + 1) and cols (m) on `st`.  `bs` holds ScanBlocks(n) words,
+// `flag` one word (set by a bad offset).
+void UnpackLists(const PackedLists& pk, uint8_t* scratch, uint64_t* bs, uint32_t* flag, uintE* rp, uintV* cols,
+                 cudaStream_t st) {
+  CK(cudaMemcpyAsync(scratch, pk.base, pk.total, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(flag, 0, sizeof(uint32_t), st));
+  PackedRowPtrs(pk, scratch, bs, rp, st);
+  UnpackRange(pk, scratch, rp, cols, flag, 0, pk.n, 0, pk.nsegs, st);
   CK(cudaGetLastError());
 }
 
@@ -1427,6 +1473,72 @@ void CheckPacked(const HostGraph& g, const PackedLists& pk) {
 
 void FailOnFlag(uint32_t flag) {
   if (flag) Fail(SME_ERR_CUDA, "packed lists are corrupt: an offset points outside the stream");
+}
+
+// Per-call packed upload into the arena, copy and expansion overlapped: the
+// header (degrees, list offsets, segment ids) and then kUploadChunks byte
+// ranges of the stream, cut at list boundaries, go over the context's copy
+// stream; the execution stream scans the degrees into row_ptrs, then, as each
+// range lands, expands its lists and builds the bitmaps of its hubs.  Hub
+// bitmaps are allocated below the copy's scratch, which is released when the
+// upload is done.  Returns the host->device bytes beyond the packed buffer.
+uint64_t UploadPackedPipelined(const HostGraph& g, const PackedLists& pk, DeviceGraph* d, DeviceContext& ctx,
+                               uint32_t* flag) {
+  auto arena_alloc = [&ctx](size_t b) { return ctx.arena.Alloc(b); };
+  const uint64_t n = pk.n;
+  const uint64_t scratch_bytes = pk.total + (uint64_t)ScanBlocks(n) * 8 + 512;
+  HubPlan hp;
+  const uint64_t room = ctx.arena.Free() > scratch_bytes ? ctx.arena.Free() - scratch_bytes : 0;
+  const bool hubs = PlanHubBitmaps(d, g, ctx.stream, arena_alloc, room, &hp);
+  const size_t mark = ctx.arena.Mark();
+  uint8_t* scratch = (uint8_t*)arena_alloc(pk.total);
+  uint64_t* bs = (uint64_t*)arena_alloc((size_t)ScanBlocks(n) * 8);
+  CK(cudaMemsetAsync(flag, 0, sizeof(uint32_t), ctx.stream));
+
+  // chunk boundaries: list ids where the stream offset passes k/K of it
+  const uint32_t* woff = reinterpret_cast<const uint32_t*>(pk.base + pk.woff_at);
+  const uint64_t* segs = reinterpret_cast<const uint64_t*>(pk.base + pk.segs_at);
+  const uint64_t lists_words = (pk.stream_bytes - 8) / 4;
+  const int K = pk.stream_bytes >= (8ULL << 20) ? kUploadChunks : 1;
+  uint64_t vb[kUploadChunks + 1];
+  vb[0] = 0;
+  vb[K] = n;
+  for (int k = 1; k < K; ++k)
+    vb[k] = std::max<uint64_t>(vb[k - 1],
+                               (uint64_t)(std::lower_bound(woff, woff + n, (uint32_t)(lists_words * k / K)) - woff));
+  auto byte_at = [&](uint64_t v) { return v < n ? (uint64_t)woff[v] * 4 : pk.stream_bytes; };
+  auto seg_at = [&](uint64_t v) {
+    return (uint64_t)(std::lower_bound(segs, segs + pk.nsegs, v << 32) - segs);
+  };
+
+  CK(cudaMemcpyAsync(scratch, pk.base, pk.stream_at, cudaMemcpyHostToDevice, ctx.copy_stream));
+  CK(cudaEventRecord(ctx.copy_ev[0], ctx.copy_stream));
+  for (int k = 0; k < K; ++k) {
+    const uint64_t b0 = k == 0 ? 0 : byte_at(vb[k]), b1 = k + 1 == K ? pk.stream_bytes : byte_at(vb[k + 1]);
+    if (b1 > b0)
+      CK(cudaMemcpyAsync(scratch + pk.stream_at + b0, pk.base + pk.stream_at + b0, b1 - b0,
+                         cudaMemcpyHostToDevice, ctx.copy_stream));
+    CK(cudaEventRecord(ctx.copy_ev[k + 1], ctx.copy_stream));
+  }
+  CK(cudaStreamWaitEvent(ctx.stream, ctx.copy_ev[0], 0));
+  PackedRowPtrs(pk, scratch, bs, d->row_ptrs, ctx.stream);
+  for (int k = 0; k < K; ++k) {
+    CK(cudaStreamWaitEvent(ctx.stream, ctx.copy_ev[k + 1], 0));
+    UnpackRange(pk, scratch, d->row_ptrs, d->cols, flag, vb[k], vb[k + 1], seg_at(vb[k]), seg_at(vb[k + 1]),
+                ctx.stream);
+    if (hubs) {
+      const std::vector<uint32_t>& H = hp.hubs();
+      const uint32_t h0 = (uint32_t)(std::lower_bound(H.begin(), H.end(), (uint32_t)vb[k]) - H.begin());
+      const uint32_t h1 = vb[k + 1] >= n ? (uint32_t)H.size()
+                                         : (uint32_t)(std::lower_bound(H.begin(), H.end(), (uint32_t)vb[k + 1]) -
+                                                      H.begin());
+      BuildHubRange(d, hp, h0, h1 - h0, ctx.stream);
+    }
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx.stream));
+  ctx.arena.Release(mark);
+  return hubs ? (uint64_t)hp.hubs().size() * 4 : 0;
 }
 }  // namespace
 
@@ -1495,20 +1607,13 @@ DeviceGraph* UploadGraphToArena(const HostGraph& g, DeviceContext& ctx, uint64_t
     if (pk) {
       CheckPacked(g, *pk);
       flag = (uint32_t*)arena_alloc(sizeof(uint32_t));
-      // the copy's scratch is released before the bitmaps take the same
-      // space: both are ordered on the context's stream
-      const size_t mark = ctx.arena.Mark();
-      uint8_t* scratch = (uint8_t*)arena_alloc(pk->total);
-      uint64_t* bs = (uint64_t*)arena_alloc((size_t)ScanBlocks(g.n) * 8);
-      UnpackLists(*pk, scratch, bs, flag, d->row_ptrs, d->cols, ctx.stream);
-      ctx.arena.Release(mark);
-      bytes = pk->total;
+      bytes = pk->total + UploadPackedPipelined(g, *pk, d, ctx, flag);
     } else {
       CK(cudaMemcpyAsync(d->row_ptrs, g.row_ptrs, (g.n + 1) * sizeof(uintE), cudaMemcpyHostToDevice, ctx.stream));
       if (g.m) CK(cudaMemcpyAsync(d->cols, g.cols, g.m * sizeof(uintV), cudaMemcpyHostToDevice, ctx.stream));
       bytes = (g.n + 1) * sizeof(uintE) + g.m * sizeof(uintV);
+      bytes += BuildHubBitmaps(d, g, ctx.stream, arena_alloc, false, ctx.arena.Free());
     }
-    bytes += BuildHubBitmaps(d, g, ctx.stream, arena_alloc, false, ctx.arena.Free());
     if (flag) {
       CK(cudaMemcpyAsync(ctx.h_pinned, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx.stream));
       CK(cudaStreamSynchronize(ctx.stream));

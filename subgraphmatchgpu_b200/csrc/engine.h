@@ -33,10 +33,15 @@ struct Arena {
   size_t Free() const { return cap - top; }
 };
 
+// Byte ranges a per-call packed upload is cut into (copy and expansion overlap).
+constexpr int kUploadChunks = 8;
+
 // Per-device execution context: stream, arena, pinned staging buffers.
 struct DeviceContext {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;             // per-call uploads
+  cudaEvent_t copy_ev[kUploadChunks + 1] = {};    // upload ranges landed
   Arena arena;
   uint64_t* h_pinned = nullptr;  // small pinned host buffer for batch bounds
   size_t pinned_words = 0;

@@ -45,9 +45,9 @@ bool HostGraph::LoopFree() const {
   return f == 1;
 }
 
-std::shared_ptr<const std::vector<uint32_t>> HostGraph::HubOrder(uint64_t min_degree) const {
+std::shared_ptr<const std::vector<uint32_t>> HostGraph::HubSelection(uint64_t min_degree, uint64_t max_hubs) const {
   std::lock_guard<std::mutex> lock(hub_mu_);
-  if (hub_order_ && hub_order_min_ == min_degree) return hub_order_;
+  if (hub_sel_ && hub_sel_min_ == min_degree && hub_sel_max_ == max_hubs) return hub_sel_;
   std::vector<std::pair<uint64_t, uint32_t>> cand;
   for (uint64_t u = 0; u < n; ++u) {
     uint64_t deg = row_ptrs[u + 1] - row_ptrs[u];
@@ -57,11 +57,14 @@ std::shared_ptr<const std::vector<uint32_t>> HostGraph::HubOrder(uint64_t min_de
                                          const std::pair<uint64_t, uint32_t>& b) {
     return a.first != b.first ? a.first > b.first : a.second < b.second;
   });
-  auto order = std::make_shared<std::vector<uint32_t>>(cand.size());
-  for (size_t i = 0; i < cand.size(); ++i) (*order)[i] = cand[i].second;
-  hub_order_ = order;
-  hub_order_min_ = min_degree;
-  return hub_order_;
+  if (cand.size() > max_hubs) cand.resize(max_hubs);
+  auto sel = std::make_shared<std::vector<uint32_t>>(cand.size());
+  for (size_t i = 0; i < cand.size(); ++i) (*sel)[i] = cand[i].second;
+  std::sort(sel->begin(), sel->end());
+  hub_sel_ = sel;
+  hub_sel_min_ = min_degree;
+  hub_sel_max_ = max_hubs;
+  return hub_sel_;
 }
 
 void HostGraph::Adopt(std::vector<uintE>&& r, std::vector<uintV>&& c) {
@@ -69,7 +72,7 @@ void HostGraph::Adopt(std::vector<uintE>&& r, std::vector<uintV>&& c) {
   packed.reset();
   {
     std::lock_guard<std::mutex> lock(hub_mu_);
-    hub_order_.reset();
+    hub_sel_.reset();
   }
   row_store = std::move(r);
   col_store = std::move(c);

@@ -83,14 +83,15 @@ struct HostGraph {
   std::shared_ptr<const PackedLists> packed;
   uint64_t MaxDegree() const;
   void Adopt(std::vector<uintE>&& r, std::vector<uintV>&& c);
-  // Vertices of degree >= min_degree, highest degree first (ties by id);
-  // computed once per graph and threshold and shared by every upload.
-  std::shared_ptr<const std::vector<uint32_t>> HubOrder(uint64_t min_degree) const;
+  // The (at most) max_hubs vertices of highest degree among those of degree
+  // >= min_degree (ties by id), sorted by id; computed once per graph and
+  // arguments and shared by every upload.
+  std::shared_ptr<const std::vector<uint32_t>> HubSelection(uint64_t min_degree, uint64_t max_hubs) const;
 
  private:
   mutable std::mutex hub_mu_;
-  mutable std::shared_ptr<const std::vector<uint32_t>> hub_order_;
-  mutable uint64_t hub_order_min_ = 0;
+  mutable std::shared_ptr<const std::vector<uint32_t>> hub_sel_;
+  mutable uint64_t hub_sel_min_ = 0, hub_sel_max_ = 0;
 };
 
 void ReadBinFile(const std::string& path, HostGraph& g);

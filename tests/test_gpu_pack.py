@@ -126,3 +126,17 @@ def test_every_vertex_a_hub(golden, monkeypatch):
         g.to_device(0)
         for q in (0, 3, 4):
             assert g.count(q, sme.GPU_GPSM_REUSE) == want[str(q)], (name, q)
+
+
+def test_per_call_packed_upload_in_ranges_counts_as_resident():
+    # an s18 graph packs to more than 8 MB, so a per-call upload is cut into
+    # ranges whose copy overlaps the expansion and the hub bitmaps
+    g = sme.Graph.rmat(18, 16, seed=18)
+    assert g.pack() >= 8 << 20
+    got = {q: g.count(q, root_begin=q, root_stride=32) for q in (0, 1, 2, 3, 4)}
+    got[0, "all"] = g.count(0)
+    g.pack(False)
+    g.to_device(0)
+    want = {q: g.count(q, root_begin=q, root_stride=32) for q in (0, 1, 2, 3, 4)}
+    want[0, "all"] = g.count(0)
+    assert got == want
