@@ -1220,16 +1220,18 @@ __global__ void k_build_bitmaps(const uintE* __restrict__ rp, const uint32_t* __
   }
 }
 
-// One hub's bitmap per CTA, built in shared memory and written out whole (no
-// memset of the bitmaps and no global atomics); for bitmaps of up to
-// kSmemBitmapBytes.
+// One hub's bitmap per CTA, built in shared memory and written out whole in
+// 16-byte stores (no memset of the bitmaps and no global atomics); for
+// bitmaps of up to kSmemBitmapBytes.  `words` is a multiple of 4.
 constexpr uint32_t kSmemBitmapBytes = 200u << 10;
 __global__ void __launch_bounds__(1024) k_build_bitmaps_smem(const uintE* __restrict__ rp,
                                                              const uint32_t* __restrict__ cols,
                                                              const uint32_t* __restrict__ hubs, uint32_t words,
                                                              uint32_t* bm) {
-  extern __shared__ uint32_t row_s[];
-  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) row_s[i] = 0;
+  extern __shared__ uint4 row_v[];
+  uint32_t* row_s = reinterpret_cast<uint32_t*>(row_v);
+  const uint32_t quads = words / 4;
+  for (uint32_t i = threadIdx.x; i < quads; i += blockDim.x) row_v[i] = make_uint4(0, 0, 0, 0);
   __syncthreads();
   const uint32_t v = hubs[blockIdx.x];
   for (uintE j = rp[v] + threadIdx.x; j < rp[v + 1]; j += blockDim.x) {
@@ -1237,8 +1239,8 @@ __global__ void __launch_bounds__(1024) k_build_bitmaps_smem(const uintE* __rest
     atomicOr(row_s + (w >> 5), 1u << (w & 31));
   }
   __syncthreads();
-  uint32_t* row = bm + (size_t)blockIdx.x * words;
-  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) row[i] = row_s[i];
+  uint4* row = reinterpret_cast<uint4*>(bm + (size_t)blockIdx.x * words);
+  for (uint32_t i = threadIdx.x; i < quads; i += blockDim.x) row[i] = row_v[i];
 }
 
 __global__ void k_set_slots(const uint32_t* __restrict__ hubs, uint32_t nh, int32_t* slot) {
@@ -1271,7 +1273,8 @@ bool PlanHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t st, Alloc a
   uint64_t budget = 1024ULL << 20;
   if (const char* e = std::getenv("SME_HUB_BITMAP_MB")) budget = std::strtoull(e, nullptr, 10) << 20;
   budget = std::min<uint64_t>(budget, room / 4);
-  const uint32_t words = (uint32_t)((g.n + 31) / 32);
+  // n bits, rounded up to whole 16-byte quads (rows start 16-byte aligned)
+  const uint32_t words = (uint32_t)(((g.n + 31) / 32 + 3) & ~uint64_t(3));
   if (budget == 0 || words == 0) return false;
   const uint64_t max_hubs = budget / ((uint64_t)words * 4);
   if (max_hubs == 0) return false;
