@@ -85,6 +85,9 @@ def parse(argv=None):
     ap.add_argument("--profile-house", type=int, default=0,
                     help="N: only count the house (LIGHT) on the bench graph over the first N roots of degree "
                          "<= hub_degree in a seeded order once (a small case for a profiler capture) and exit")
+    ap.add_argument("--profile-upload", type=int, default=0,
+                    help="N: only run N counts of the first diamond step on the bench graph held packed in host "
+                         "memory (every call uploads and expands it; a small case for a profiler capture) and exit")
     ap.add_argument("--profile-s22", default="",
                     help="BEGIN:END:STRIDE: only count the 4-clique of the degree-oriented R-MAT s22 graph over "
                          "roots BEGIN, BEGIN+STRIDE, ... < END once (a small case for a profiler capture), print "
@@ -760,6 +763,53 @@ def profile_house(args):
                       "hot_launches": s.hot_launches, "phase_ms": list(s.phase_ms)}), flush=True)
 
 
+def profile_upload(args):
+    """N counts of the first diamond step on the bench graph, not resident and
+    held packed: each call copies the packed lists in ranges, expands them and
+    builds the hub bitmaps before counting (the upload kernels for a profiler
+    capture)."""
+    import subgraphmatchgpu_b200 as sme
+    g = engine_graph(args)
+    rp, _ = g.csr()
+    packed = g.pack()
+    q, roots = next((q, r) for q, r in make_steps(rp, args, 3) if q == 2)
+    out = []
+    for _ in range(args.profile_upload):
+        c = g.count(q, sme.GPU_LIGHT, roots=roots)
+        s = sme.last_stats()
+        out.append({"instances": c, "elapsed_ms": s.elapsed_ms, "device_ms": s.device_ms, "h2d_bytes": s.h2d_bytes})
+    print(json.dumps({"packed_bytes": packed, "calls": out}), flush=True)
+
+
+def bench_noalloc(device):
+    """sme_count_noalloc beside sme_count on one resident R-MAT graph: the
+    allocation-free path trades parallelism for its fixed scratch array."""
+    import ctypes
+    import subgraphmatchgpu_b200 as sme
+    g = sme.Graph.rmat(16, 16, seed=16)
+    g.to_device(device)
+    d_rp, d_cl = g.device_arrays(device)
+    out = {"graph": "R-MAT s16 ef16 seed 16 (library generator)", "n": g.n, "m": g.m,
+           "max_degree": g.info()[2], "queries": {}}
+    # the triangle only: on this graph the 4-clique takes the allocation-free
+    # path about 10 s and the 4-cycle about 100 s (sme_count: 11 and 167 ms)
+    for q in (0,):
+        g.count(q, device=device)
+        t0 = time.perf_counter()
+        want = g.count(q, device=device)
+        t_count = time.perf_counter() - t0
+        got = ctypes.c_uint64()
+        sme.lib().sme_count_noalloc(d_rp, d_cl, g.n, q, ctypes.byref(got))
+        t0 = time.perf_counter()
+        st = sme.lib().sme_count_noalloc(d_rp, d_cl, g.n, q, ctypes.byref(got))
+        t_noalloc = time.perf_counter() - t0
+        out["queries"][QUERY_NAMES.get(q, str(q))] = {
+            "sme_count_ms": round(t_count * 1e3, 3), "sme_count_noalloc_ms": round(t_noalloc * 1e3, 3),
+            "status": st, "counts_equal": st == 0 and got.value == want, "instances": want}
+    g.release_device()
+    return out
+
+
 def profile_s22(args):
     """One count of the 4-clique over a root range of the degree-oriented
     R-MAT s22 ef16 graph (the graph of the s22 legs), resident, with the
@@ -789,6 +839,8 @@ def main():
         return profile_s22(args)
     if args.profile_house:
         return profile_house(args)
+    if args.profile_upload:
+        return profile_upload(args)
 
     import torch
     import subgraphmatchgpu_b200 as sme
@@ -948,6 +1000,10 @@ def main():
                     legs[name] = fn(args, local)
                 except Exception as ex:
                     legs[name] = {"error": f"{type(ex).__name__}: {ex}"}
+            try:
+                legs["noalloc"] = bench_noalloc(local)
+            except Exception as ex:
+                legs["noalloc"] = {"error": f"{type(ex).__name__}: {ex}"}
         if not args.no_s22:
             try:
                 legs["s22"] = bench_s22(args, local, tune, peak)
