@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
     }
     BoundsT<NEX> bd = MakeBounds<NEX>(s.cond, F, p);
     uint32_t r0 = 0, r1 = 0;
-    if (nl > 0) Range(L[0], N[0], bd, r0, r1);
+    if (nl > 0) WarpRange(L[0], N[0], bd, r0, r1);
     if (DEFER && nl == 2 && r1 - r0 >= hv.min_len) {
       uint32_t slot = 0;
       if (lane == 0) slot = atomicAdd(hv.q, 1u);
@@ -476,6 +476,160 @@ __global__ void __launch_bounds__(WARP_BLOCK, MINB) k_compute(
   }
   if (lane == 0 && bytes) atomicAdd(acc + 1, bytes);
   if (MAPPED && lane == 0 && hits) atomicAdd(acc + 5, hits);
+}
+
+// ---- intersection of the root's list with one other list -------------------
+// Steps that intersect exactly two adjacency lists, one of them the list of
+// the plan's first vertex (the root of the task: the 4-cycle's and the
+// triangle's count steps, the diamond's path count, the 4-clique's second
+// level).  The frontier keeps the paths of a root together (materialisation
+// preserves the parents' order), so a CTA holds the root's list as an n-bit
+// bitmap in shared memory and rebuilds it only when the root changes between
+// runs of paths.  Per path a warp then takes the cheapest of: walking the
+// other list's clipped range and testing each element in the shared bitmap
+// (no search at all), walking the root's clipped range and testing the other
+// vertex's hub bitmap (one load each), or walking the root's clipped range
+// with a binary search in the other list (the warp kernel's way).  Costs are
+// compared in warp iterations, a binary search counting log2 of the list.
+// Results equal k_compute's: MODE 0 writes the sorted set (both walks visit
+// ascending values), MODE 1 counts, MODE 2 stores the count.  CTAs take
+// chunks of RM_CHUNK paths from a counter.
+constexpr int RM_THREADS = 1024;
+constexpr int RM_WARPS = RM_THREADS / 32;
+constexpr uint32_t RM_CHUNK = 2048;
+constexpr uint32_t kRootMapMaxBytes = 200u << 10;  // bitmaps up to n = 1 638 400
+constexpr uint32_t kNoRoot = 0xFFFFFFFFu;
+
+template <int MODE, int NEX>
+__global__ void __launch_bounds__(RM_THREADS, 2) k_compute_rootmap(
+    DFront F, DStep s, DGraph G, int ru, int other, const uint64_t* __restrict__ est_incl, uint32_t b0,
+    uint64_t* out_ptr, uint32_t* out_cnt, uint32_t* out_data, uint64_t out_cap, unsigned long long* acc,
+    uint32_t* err, uint32_t* next_chunk, uint32_t words) {
+  extern __shared__ uint32_t rmap[];
+  __shared__ uint32_t s_chunk, s_end;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1;
+  for (uint32_t i = threadIdx.x; i < words; i += RM_THREADS) rmap[i] = 0;
+  unsigned long long local = 0, bytes = 0;
+  const uint64_t base = (MODE == 0 && b0 > 0) ? est_incl[b0 - 1] : 0;
+  const uint32_t* rootcol = F.inst[ru];
+  const uint32_t* othercol = F.inst[other];
+  uint32_t cur_root = kNoRoot;
+  __syncthreads();
+  while (true) {
+    if (threadIdx.x == 0) s_chunk = atomicAdd(next_chunk, 1u);
+    __syncthreads();
+    const uint64_t c0 = (uint64_t)s_chunk * RM_CHUNK;
+    __syncthreads();  // s_chunk is rewritten only after the next barrier pair
+    if (c0 >= F.P) break;
+    const uint32_t c1 = (uint32_t)(c0 + RM_CHUNK < F.P ? c0 + RM_CHUNK : F.P);
+    uint32_t p = (uint32_t)c0;
+    while (p < c1) {
+      const uint32_t r = __ldg(rootcol + p);
+      if (threadIdx.x == 0) s_end = c1;
+      __syncthreads();
+      for (uint32_t q = p + threadIdx.x; q < c1; q += RM_THREADS)
+        if (__ldg(rootcol + q) != r) {
+          atomicMin(&s_end, q);
+          break;
+        }
+      __syncthreads();
+      const uint32_t e = s_end;
+      if (r != cur_root) {
+        const uint32_t* L;
+        uint32_t N;
+        if (cur_root != kNoRoot) {
+          AdjList(G, cur_root, L, N);
+          for (uint32_t i = threadIdx.x; i < N; i += RM_THREADS) rmap[__ldg(L + i) >> 5] = 0;
+          __syncthreads();
+        }
+        AdjList(G, r, L, N);
+        for (uint32_t i = threadIdx.x; i < N; i += RM_THREADS) {
+          const uint32_t x = __ldg(L + i);
+          atomicOr(rmap + (x >> 5), 1u << (x & 31));
+        }
+        __syncthreads();
+        cur_root = r;
+      }
+      const uint32_t* Lr;
+      uint32_t Nr;
+      AdjList(G, r, Lr, Nr);
+      for (uint32_t pp = p + wid; pp < e; pp += RM_WARPS) {
+        const uint32_t v = __ldg(othercol + pp);
+        const uint32_t* Lv;
+        uint32_t Nv;
+        AdjList(G, v, Lv, Nv);
+        const uint32_t* Bv = HubBitmap(G, v);
+        BoundsT<NEX> bd = MakeBounds<NEX>(s.cond, F, pp);
+        uint32_t a0, a1, v0, v1;
+        WarpRange(Lr, Nr, bd, a0, a1);
+        WarpRange(Lv, Nv, bd, v0, v1);
+        // algorithmic bytes as the warp kernel counts them: the smaller
+        // list is the pivot, its clipped range read and tested once
+        if (lane == 0) bytes += 24ULL + 8ULL * (Nv < Nr ? v1 - v0 : a1 - a0);
+        const uint32_t wv = (v1 - v0 + 31) >> 5, wr = (a1 - a0 + 31) >> 5;
+        int how = 0;  // 0: walk v's range, test the shared bitmap
+        if (Bv) {
+          if (wr < wv) how = 1;  // walk the root's range, test v's hub bitmap
+        } else {
+          const uint32_t lg = 32 - __clz(Nv | 1u);
+          if (wr * lg < wv) how = 2;  // walk the root's range, search v's list
+        }
+        const uint32_t* W = how == 0 ? Lv : Lr;
+        const uint32_t w0 = how == 0 ? v0 : a0, w1 = how == 0 ? v1 : a1;
+        uint64_t out_off = 0;
+        if (MODE == 0) out_off = (pp + b0 == 0 ? 0 : est_incl[pp + b0 - 1]) - base;
+        uint32_t cur = 0, written = 0;
+        for (uint32_t bi = w0; bi < w1; bi += 32) {
+          const uint32_t i = bi + lane;
+          bool ok = i < w1;
+          const uint32_t x = ok ? __ldg(W + i) : 0;
+#pragma unroll
+          for (int k = 0; k < NEX; ++k)
+            if (k < bd.nne && x == bd.ne[k]) ok = false;
+          if (ok) {
+            if (how == 0) {
+              ok = (rmap[x >> 5] >> (x & 31)) & 1u;
+            } else if (how == 1) {
+              ok = BitTest(Bv, x);
+            } else {
+              const uint32_t pos = cur + LowerBound(Lv + cur, Nv - cur, x);
+              cur = pos;
+              ok = pos < Nv && __ldg(Lv + pos) == x;
+            }
+          }
+          const unsigned mask = __ballot_sync(FULL, ok);
+          if (MODE == 0) {
+            const uint64_t o = out_off + written + __popc(mask & lt);
+            if (ok) {
+              if (o < out_cap) out_data[o] = x;
+              else atomicOr(err, ENGINE_ERR_BOUNDS);
+            }
+          } else if (MODE == 1 && lane == 0) {
+            local += __popc(mask);
+          }
+          written += __popc(mask);
+        }
+        if (lane == 0) {
+          if (MODE == 0) {
+            out_ptr[pp] = (uint64_t)(out_data + out_off);
+            out_cnt[pp] = written;
+            bytes += 4ULL * written;
+          } else if (MODE == 2) {
+            out_ptr[pp] = 0;
+            out_cnt[pp] = written;
+          }
+        }
+      }
+      __syncthreads();  // the bitmap may change for the next run
+      p = e;
+    }
+  }
+  if (MODE == 1) {
+    local = WarpSum(local);
+    if (lane == 0 && local) atomicAdd(acc, local);
+  }
+  if (lane == 0 && bytes) atomicAdd(acc + 1, bytes);
 }
 
 // ---- intersection, one CTA per long-pivot path ----------------------------
@@ -1942,8 +2096,37 @@ class Executor {
                                                                       err);
   }
 
+  // The root's list as a shared-memory bitmap (k_compute_rootmap), the
+  // attribute for its dynamic shared memory set once per device.
+  template <int MODE, int NEX>
+  void LaunchRootMapAs(int ru, int other, const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est,
+                       uint32_t b0, uint64_t* ptr, uint32_t* cnt, uint32_t* data, uint64_t cap,
+                       unsigned long long* acc, uint32_t* err) {
+    static bool set[64] = {false};
+    const int d = ctx_.device;
+    if (d >= 0 && d < 64 && !set[d]) {
+      CK(cudaFuncSetAttribute(k_compute_rootmap<MODE, NEX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kRootMapMaxBytes));
+      set[d] = true;
+    }
+    const uint32_t words = (uint32_t)((g_.n + 31) / 32);
+    const size_t bytes = (size_t)words * 4;
+    const size_t mark = A_.Mark();
+    uint32_t* next = (uint32_t*)A_.Alloc(4);
+    CK(cudaMemsetAsync(next, 0, 4, st_));
+    // two CTAs of 1024 threads per SM while two bitmaps fit shared memory
+    const uint64_t per_sm = bytes <= (112u << 10) ? 2 : 1;
+    const unsigned grid =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(sms_ * per_sm, (F.P + RM_CHUNK - 1) / RM_CHUNK));
+    k_compute_rootmap<MODE, NEX><<<grid, RM_THREADS, bytes, st_>>>(F, ds, G, ru, other, est, b0, ptr, cnt, data,
+                                                                    cap, acc, err, next, words);
+    A_.Release(mark);
+  }
+
   // Intersection launch: warp per path, specialised (granularity 0 auto, 3),
-  // warp per path generic (1) or flattened over 32 paths per warp (2).
+  // warp per path generic (1) or flattened over 32 paths per warp (2); in the
+  // auto launches, a two-list step that reads the root's list takes
+  // k_compute_rootmap (SME_ROOT_MAP=0 turns it off).
   template <int MODE>
   void Compute(const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est, uint32_t b0, uint64_t* ptr,
                uint32_t* cnt, uint32_t* data, uint64_t cap, const uint32_t* perm = nullptr) {
@@ -1954,7 +2137,26 @@ class Executor {
     const int nlists = ds.nconn + (ds.reuse >= 0 ? 1 : 0);
     bool has_ne = false;
     for (int i = 0; i < ds.cond.n; ++i) has_ne |= ds.cond.op[i] == 2;
-    if (MODE == 1 && perm && ds.msrc < 0 && (gran == 0 || gran == 3) && nlists <= 3) {
+    const int ru = prog_.steps[0].u;
+    int ri = -1;
+    for (int i = 0; i < ds.nconn; ++i)
+      if (ds.conn[i] == ru) ri = i;
+    // the bitmap pays only where a root has many paths (its rebuild and the
+    // CTA's barriers are per run of paths): three or more materialised
+    // vertices (the 4-cycle's count step, not the diamond's or the
+    // 4-clique's second level, measured 3.4x and 2.2x slower there)
+    int nmat = 0;
+    for (int v = 0; v < MAXV; ++v) nmat += F.inst[v] != nullptr;
+    const bool rootmap = root_map_ && nmat >= 3 && !perm && ds.msrc < 0 && ds.reuse < 0 && ds.nconn == 2 && ri >= 0 &&
+                         (gran == 0 || gran == 3) && (MODE != 1 || ds.with_u < 0) && !G.coff && g_.n > 0 &&
+                         (g_.n + 31) / 32 * 4 <= kRootMapMaxBytes && F.inst[ru] && F.inst[ds.conn[1 - ri]];
+    if (rootmap) {
+      const int other = ds.conn[1 - ri];
+      if (has_ne)
+        LaunchRootMapAs<MODE, MAXV>(ru, other, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+      else
+        LaunchRootMapAs<MODE, 0>(ru, other, F, ds, G, est, b0, ptr, cnt, data, cap, acc, err);
+    } else if (MODE == 1 && perm && ds.msrc < 0 && (gran == 0 || gran == 3) && nlists <= 3) {
       // count step, paths taken hub by hub (see k_hub_hist)
       if constexpr (MODE == 1) {
         DHeavy hv{};
@@ -2039,6 +2241,7 @@ class Executor {
   uint32_t heavy_min_ = 2048;  // granularity 4: shortest pivot that gets a CTA
   bool group_by_hub_ = false;  // count steps take their paths hub by hub
   bool use_bitmaps_ = true;
+  bool root_map_ = true;  // two-list steps on the root's list: k_compute_rootmap
 
  private:
 
@@ -2337,6 +2540,7 @@ RunResult RunProgram(const Program& prog, const DeviceGraph& g, DeviceContext& c
   ex.use_bitmaps_ = !(tuning & 0x100);
   if (const char* e = std::getenv("SME_HEAVY_PIVOT")) ex.heavy_min_ = (uint32_t)std::max(32L, std::atol(e));
   if (const char* e = std::getenv("SME_GROUP_BY_HUB")) ex.group_by_hub_ = std::atoi(e) != 0;
+  if (const char* e = std::getenv("SME_ROOT_MAP")) ex.root_map_ = std::atoi(e) != 0;
   return ex.Run(t);
 }
 

@@ -188,6 +188,41 @@ __device__ __forceinline__ void Range(const uint32_t* a, uint32_t n, const Bound
   if (r1 < r0) r1 = r0;
 }
 
+// First index i in a[0,n) with a[i] >= x, found by the whole warp (every lane
+// calls it with the same arguments): each round the 32 lanes probe 32 evenly
+// spaced elements and a ballot narrows the range 32-fold, so a list of up to
+// 1024 elements takes two dependent rounds instead of ten loads in a row.
+__device__ __forceinline__ uint32_t WarpLowerBound(const uint32_t* __restrict__ a, uint32_t n, uint32_t x) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t lo = 0, len = n;  // the answer lies in [lo, lo + len]
+  while (len > 32) {
+    const uint32_t step = (len + 31) / 32;
+    const uint32_t idx = lo + lane * step;
+    const bool lt = idx < lo + len && __ldg(a + idx) < x;
+    const uint32_t c = __popc(__ballot_sync(0xffffffffu, lt));  // samples below x: a prefix
+    if (c == 0) return lo;
+    const uint32_t nlo = lo + (c - 1) * step + 1;
+    const uint32_t nhi = min(lo + c * step, lo + len);
+    lo = nlo;
+    len = nhi - nlo;
+  }
+  const bool lt = lane < len && __ldg(a + lo + lane) < x;
+  return lo + __popc(__ballot_sync(0xffffffffu, lt));
+}
+
+// Range with the warp's lower bound (same result; warp-uniform arguments).
+template <int NE>
+__device__ __forceinline__ void WarpRange(const uint32_t* a, uint32_t n, const BoundsT<NE>& b, uint32_t& r0,
+                                          uint32_t& r1) {
+  if (b.lo >= b.hi) {
+    r0 = r1 = 0;
+    return;
+  }
+  r0 = b.lo == 0 ? 0 : (b.lo > 0xffffffffULL ? n : WarpLowerBound(a, n, (uint32_t)b.lo));
+  r1 = b.hi > 0xffffffffULL ? n : WarpLowerBound(a, n, (uint32_t)b.hi);
+  if (r1 < r0) r1 = r0;
+}
+
 // Positions (ascending) of excluded values present in a[r0,r1).
 template <int NE>
 __device__ __forceinline__ int Exclusions(const uint32_t* a, uint32_t r0, uint32_t r1, const BoundsT<NE>& b,

@@ -49,6 +49,29 @@ def test_intersection_granularities(graphs, golden, gran):
         assert np.array_equal(got, O.enumerate_sorted(rp, cl, q))
 
 
+@pytest.mark.parametrize("root_map", ["0", "1"])
+def test_root_list_bitmap_and_warp_kernel_agree(graphs, golden, root_map, monkeypatch):
+    # two-list steps on the root's list run k_compute_rootmap by default
+    # (the root's list as a shared-memory bitmap); SME_ROOT_MAP=0 sends them
+    # to the warp-per-path kernel.  Both give the reference's counts, and
+    # the same sorted instances (write steps).
+    monkeypatch.setenv("SME_ROOT_MAP", root_map)
+    for name in ("rmat_s12_ef8", "ba_n600_m4", "er_n600_d8", "k20"):
+        for q, want in golden[name]["counts"].items():
+            if want > GPU_LIMIT:
+                continue
+            for algo in ALGOS:
+                got = graphs[name].count(int(q), algo)
+                assert got == want, (name, q, algo, root_map, got, want)
+    for name in ("er_n64_d12", "ba_n600_m4"):
+        rp, cl = O.read_bin(golden_graph_path(name))
+        for q in (0, 1, 2, 3, 7):
+            want = O.enumerate_sorted(rp, cl, q)
+            for algo in ALGOS:
+                got = O.sort_rows(graphs[name].enumerate(q, algo))
+                assert got.shape == want.shape and np.array_equal(got, want), (name, q, algo, root_map)
+
+
 @pytest.mark.parametrize("threshold", ["32", "256"])
 def test_long_pivot_paths_on_a_cta_each(graphs, golden, threshold, monkeypatch):
     # granularity 4: two-list steps hand paths whose clipped pivot holds at
