@@ -1058,15 +1058,117 @@ __global__ void k_mat_count(DFront F, int u, DCond c, uint64_t* cnt) {
 // Expands each path's valid candidates into child rows: materialised columns
 // (broadcast from the parent) plus the new vertex, and the set index of every
 // live candidate set (Materialize, src/gpu/impl/light/op/LIGHTMaterialize.cuh:23-162,
-// fused: expand + filter + compact + per-column gather in one pass).
+// fused: expand + filter + compact + per-column gather in one pass).  Work is
+// cut by child rows, not by parents: a warp takes kMatChunk consecutive rows,
+// finds the parent of the first one with a warp-cooperative search over the
+// inclusive child counts, and walks forward through the parents the chunk
+// covers; the k-th child of a parent is its k-th candidate in the clipped
+// range that is not excluded.  A parent with tens of thousands of children
+// (a hub's list) is spread over many warps instead of holding one.  Only
+// parents of more than `big` children are expanded here (the rest, whose
+// per-parent set-up a chunk would serialise, take k_mat_write); the parents
+// a chunk covers are scanned 32 at a time, one coalesced load per lane.
+constexpr uint32_t kMatChunk = 1024;
+constexpr uint64_t kMatBig = 2048;
+
+// First p in [0, n) with a[p] > c, by the whole warp (`a` non-decreasing).
+__device__ __forceinline__ uint32_t WarpUpperBound64(const uint64_t* __restrict__ a, uint32_t n, uint64_t c) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t lo = 0, len = n;
+  while (len > 32) {
+    const uint32_t step = (len + 31) / 32;
+    const uint32_t idx = lo + lane * step;
+    const bool le = idx < lo + len && __ldg(a + idx) <= c;
+    const uint32_t k = __popc(__ballot_sync(0xffffffffu, le));
+    if (k == 0) return lo;
+    const uint32_t nlo = lo + (k - 1) * step + 1;
+    const uint32_t nhi = min(lo + k * step, lo + len);
+    lo = nlo;
+    len = nhi - nlo;
+  }
+  const bool le = lane < len && __ldg(a + lo + lane) <= c;
+  return lo + __popc(__ballot_sync(0xffffffffu, le));
+}
+
+__global__ void __launch_bounds__(WARP_BLOCK) k_mat_write_big(DFront F, DCond c, DMatOut o,
+                                                              const uint64_t* __restrict__ incl,
+                                                              uint64_t total, uint64_t big, uint32_t* err) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const int u = o.u;
+  for (uint64_t c0 = (uint64_t)gw * kMatChunk; c0 < total; c0 += (uint64_t)nw * kMatChunk) {
+    const uint64_t c1 = c0 + kMatChunk < total ? c0 + kMatChunk : total;
+    // the parents overlapping [c0, c1) start at the parent of row c0; they
+    // are scanned 32 at a time and only the large ones expanded
+    uint32_t p = WarpUpperBound64(incl, F.P, c0);
+    while (p < F.P) {
+      const uint32_t q = p + lane;
+      bool cand = false, past = false;
+      if (q < F.P) {
+        const uint64_t qe = __ldg(incl + q), qo = q == 0 ? 0 : __ldg(incl + q - 1);
+        past = qo >= c1;
+        cand = !past && qe - qo > big;  // qe > c0 holds for every q at or after the first parent
+      }
+      const unsigned mp = __ballot_sync(FULL, past);
+      unsigned todo = __ballot_sync(FULL, cand);
+      if (mp) todo &= (1u << (__ffs(mp) - 1)) - 1;
+      while (todo) {
+        const uint32_t pp = p + (__ffs(todo) - 1);
+        todo &= todo - 1;
+        const uint64_t off = pp == 0 ? 0 : __ldg(incl + pp - 1);
+        const uint64_t end = __ldg(incl + pp);
+        const uint32_t* a;
+        uint32_t n;
+        GetSet(F, u, pp, a, n);
+        Bounds bd = MakeBounds(c, F, pp);
+        uint32_t r0, r1, ex[MAXV];
+        WarpRange(a, n, bd, r0, r1);
+        int ne = Exclusions(a, r0, r1, bd, ex);
+        uint32_t vals[MAXV], idx[MAXV];
+#pragma unroll
+        for (int i = 0; i < MAXV; ++i) {
+          vals[i] = 0;
+          idx[i] = 0;
+          if (i < o.nmat && o.mat[i] != u) vals[i] = F.inst[o.mat[i]][pp];
+          if (i < o.nsets) idx[i] = SetIndex(F, o.sets[i], pp);
+        }
+        const uint64_t s0 = off > c0 ? off : c0, s1 = end < c1 ? end : c1;
+        for (uint64_t w = s0 + lane; w < s1; w += 32) {
+          // the (w - off)-th candidate of [r0, r1) that is not excluded
+          uint32_t j = r0 + (uint32_t)(w - off);
+#pragma unroll
+          for (int k = 0; k < MAXV; ++k)
+            if (k < ne && ex[k] <= j) ++j;
+          if (j >= r1) {
+            atomicOr(err, ENGINE_ERR_BOUNDS);
+            continue;
+          }
+          const uint32_t x = __ldg(a + j);
+#pragma unroll
+          for (int i = 0; i < MAXV; ++i) {
+            if (i < o.nmat) o.inst[o.mat[i]][w] = o.mat[i] == u ? x : vals[i];
+            if (i < o.nsets) o.cidx[o.sets[i]][w] = idx[i];
+          }
+        }
+      }
+      if (mp) break;
+      p += 32;
+    }
+  }
+}
+
+// Parents of at most `big` children: one warp each (the large ones are
+// k_mat_write_big's).
 __global__ void __launch_bounds__(WARP_BLOCK) k_mat_write(DFront F, DCond c, DMatOut o,
                                                           const uint64_t* __restrict__ incl,
-                                                          uint64_t total, uint32_t* err) {
+                                                          uint64_t total, uint64_t big, uint32_t* err) {
   const int lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   const int u = o.u;
   for (uint32_t p = gw; p < F.P; p += nw) {
+    if ((p == 0 ? incl[0] : incl[p] - incl[p - 1]) > big) continue;  // k_mat_write_big's
     const uint32_t* a;
     uint32_t n;
     GetSet(F, u, p, a, n);
@@ -2502,7 +2604,10 @@ class Executor {
             o.sets[i] = s.sets_after[i];
             o.cidx[s.sets_after[i]] = (uint32_t*)A_.Alloc(C * 4);
           }
-          k_mat_write<<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, dc, o, cnt, C, err);
+          k_mat_write<<<WarpGrid(Pb), WARP_BLOCK, 0, st_>>>(Fb, dc, o, cnt, C, kMatBig, err);
+          k_mat_write_big<<<WarpGrid((C + kMatChunk - 1) / kMatChunk), WARP_BLOCK, 0, st_>>>(Fb, dc, o, cnt, C,
+                                                                                             kMatBig, err);
+          Launched();
           TimerStop(tm, kPhaseMaterialize);
           Launched();
           DFront Fn{};
