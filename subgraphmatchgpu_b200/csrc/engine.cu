@@ -16,6 +16,7 @@
 //     an adjacency list or of an earlier set is not copied;
 //   * counts accumulate on the device; the host reads one uint64 at the end.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <string>
@@ -2164,11 +2165,13 @@ class Executor {
   template <int MODE>
   size_t CtaWindowBytes() {
     constexpr size_t kBytes = 64 << 10;
-    static bool set[64] = {false};
+    // per device, once (server slots on several host threads may race here;
+    // setting the attribute twice is harmless)
+    static std::atomic<bool> set[64];
     const int d = ctx_.device;
-    if (d >= 0 && d < 64 && !set[d]) {
+    if (d >= 0 && d < 64 && !set[d].load(std::memory_order_acquire)) {
       CK(cudaFuncSetAttribute(k_compute_cta<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBytes));
-      set[d] = true;
+      set[d].store(true, std::memory_order_release);
     }
     return kBytes;
   }
@@ -2204,12 +2207,14 @@ class Executor {
   void LaunchRootMapAs(int ru, int other, const DFront& F, const DStep& ds, const DGraph& G, const uint64_t* est,
                        uint32_t b0, uint64_t* ptr, uint32_t* cnt, uint32_t* data, uint64_t cap,
                        unsigned long long* acc, uint32_t* err) {
-    static bool set[64] = {false};
+    // per device, once (server slots on several host threads may race here;
+    // setting the attribute twice is harmless)
+    static std::atomic<bool> set[64];
     const int d = ctx_.device;
-    if (d >= 0 && d < 64 && !set[d]) {
+    if (d >= 0 && d < 64 && !set[d].load(std::memory_order_acquire)) {
       CK(cudaFuncSetAttribute(k_compute_rootmap<MODE, NEX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)kRootMapMaxBytes));
-      set[d] = true;
+      set[d].store(true, std::memory_order_release);
     }
     const uint32_t words = (uint32_t)((g_.n + 31) / 32);
     const size_t bytes = (size_t)words * 4;
