@@ -561,6 +561,7 @@ __global__ void __launch_bounds__(RM_THREADS, 2) k_compute_rootmap(
         uint32_t Nv;
         AdjList(G, v, Lv, Nv);
         const uint32_t* Bv = HubBitmap(G, v);
+        const uint32_t* Cv = HubCoarse(G, v);
         BoundsT<NEX> bd = MakeBounds<NEX>(s.cond, F, pp);
         uint32_t a0, a1, v0, v1;
         WarpRange(Lr, Nr, bd, a0, a1);
@@ -592,7 +593,7 @@ __global__ void __launch_bounds__(RM_THREADS, 2) k_compute_rootmap(
             if (how == 0) {
               ok = (rmap[x >> 5] >> (x & 31)) & 1u;
             } else if (how == 1) {
-              ok = BitTest(Bv, x);
+              ok = BitTest2(Bv, Cv, x);
             } else {
               const uint32_t pos = cur + LowerBound(Lv + cur, Nv - cur, x);
               cur = pos;
@@ -1484,7 +1485,7 @@ constexpr uint32_t kSmemBitmapBytes = 200u << 10;
 __global__ void __launch_bounds__(1024) k_build_bitmaps_smem(const uintE* __restrict__ rp,
                                                              const uint32_t* __restrict__ cols,
                                                              const uint32_t* __restrict__ hubs, uint32_t words,
-                                                             uint32_t* bm) {
+                                                             uint32_t* bm, uint32_t* coarse, uint32_t cwords) {
   extern __shared__ uint4 row_v[];
   uint32_t* row_s = reinterpret_cast<uint32_t*>(row_v);
   const uint32_t quads = words / 4;
@@ -1498,6 +1499,16 @@ __global__ void __launch_bounds__(1024) k_build_bitmaps_smem(const uintE* __rest
   __syncthreads();
   uint4* row = reinterpret_cast<uint4*>(bm + (size_t)blockIdx.x * words);
   for (uint32_t i = threadIdx.x; i < quads; i += blockDim.x) row[i] = row_v[i];
+  // coarse row: bit b of word cw set when bitmap word 32 cw + b is not zero
+  uint32_t* crow = coarse + (size_t)blockIdx.x * cwords;
+  for (uint32_t cw = threadIdx.x; cw < cwords; cw += blockDim.x) {
+    uint32_t bits = 0;
+    for (uint32_t b = 0; b < 32; ++b) {
+      const uint32_t wi = cw * 32 + b;
+      if (wi < words && row_s[wi]) bits |= 1u << b;
+    }
+    crow[cw] = bits;
+  }
 }
 
 __global__ void k_set_slots(const uint32_t* __restrict__ hubs, uint32_t nh, int32_t* slot) {
@@ -1542,6 +1553,10 @@ bool PlanHubBitmaps(DeviceGraph* d, const HostGraph& g, cudaStream_t st, Alloc a
   hp->smem = (uint64_t)words * 4 <= kSmemBitmapBytes;
   d->hub_slot = (int32_t*)alloc(g.n * sizeof(int32_t));
   d->bitmaps = (uint32_t*)alloc((size_t)nh * words * 4);
+  if (hp->smem) {  // built beside the bitmap by the shared-memory builder
+    d->cwords = (words + 31) / 32;
+    d->coarse = (uint32_t*)alloc((size_t)nh * d->cwords * 4);
+  }
   hp->d_hubs = (uint32_t*)alloc((size_t)nh * 4);
   CK(cudaMemcpyAsync(hp->d_hubs, hp->sel->data(), (size_t)nh * 4, cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync(d->hub_slot, 0xFF, g.n * sizeof(int32_t), st));
@@ -1558,8 +1573,9 @@ void BuildHubRange(const DeviceGraph* d, const HubPlan& hp, uint32_t first, uint
   if (hp.smem) {
     CK(cudaFuncSetAttribute(k_build_bitmaps_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)kSmemBitmapBytes));
-    k_build_bitmaps_smem<<<count, 1024, (size_t)hp.words * 4, st>>>(d->row_ptrs, d->cols, hp.d_hubs + first,
-                                                                     hp.words, d->bitmaps + (size_t)first * hp.words);
+    k_build_bitmaps_smem<<<count, 1024, (size_t)hp.words * 4, st>>>(
+        d->row_ptrs, d->cols, hp.d_hubs + first, hp.words, d->bitmaps + (size_t)first * hp.words,
+        d->coarse + (size_t)first * d->cwords, d->cwords);
   } else {
     k_build_bitmaps<<<count, 256, 0, st>>>(d->row_ptrs, d->cols, hp.d_hubs + first, hp.words,
                                            d->bitmaps + (size_t)first * hp.words);
@@ -1899,6 +1915,7 @@ void FreeDeviceGraph(DeviceGraph* d) {
   if (d->cols && !d->host_mapped) cudaFree(d->cols);
   if (d->hub_slot) cudaFree(d->hub_slot);
   if (d->bitmaps) cudaFree(d->bitmaps);
+  if (d->coarse) cudaFree(d->coarse);
   delete d;
 }
 
@@ -2056,8 +2073,9 @@ class Executor {
   // while deeper levels use candidate sets that point into it).
   // The resident graph with its hub bitmaps (`use_bitmaps_` false: lists only).
   DGraph Resident() const {
-    if (use_bitmaps_ && g_.hub_slot) return DGraph{g_.row_ptrs, g_.cols, g_.hub_slot, g_.bitmaps, g_.words};
-    return DGraph{g_.row_ptrs, g_.cols, nullptr, nullptr, 0};
+    if (use_bitmaps_ && g_.hub_slot)
+      return DGraph{g_.row_ptrs, g_.cols, g_.hub_slot, g_.bitmaps, g_.words, nullptr, g_.coarse, g_.cwords};
+    return DGraph{g_.row_ptrs, g_.cols, nullptr, nullptr, 0, nullptr, nullptr, 0};
   }
 
   DGraph LoadSubgraph(const DFront& Fb, const DStep& ds) {
@@ -2097,7 +2115,7 @@ class Executor {
     }
     A_.Release(mark);
     TimerStop(tl, kPhaseExternal);
-    return DGraph{g_.row_ptrs, ext_cache_, nullptr, nullptr, 0, ext_off_};
+    return DGraph{g_.row_ptrs, ext_cache_, nullptr, nullptr, 0, ext_off_, nullptr, 0};
   }
 
   uint64_t ReadU32(const unsigned int* d) {

@@ -19,6 +19,10 @@ struct DeviceGraph {
   int32_t* hub_slot = nullptr;  // per vertex: bitmap slot or -1
   uint32_t* bitmaps = nullptr;  // nhubs x words
   uint32_t words = 0, nhubs = 0;
+  // per hub, one bit per 32-vertex block of its bitmap (set: the block holds
+  // a neighbour); nhubs x cwords, null when not built
+  uint32_t* coarse = nullptr;
+  uint32_t cwords = 0;
 };
 
 // Stack allocator over one device allocation.  Levels are processed depth

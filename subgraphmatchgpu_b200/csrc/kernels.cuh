@@ -94,6 +94,9 @@ struct DGraph {
   // external mode: the lists live in a device cache; coff[v] is v's first
   // element in `cols` (null: cols is the CSR and rp indexes it)
   const uint64_t* coff;
+  // per hub, one bit per 32-vertex block of its bitmap (null: none)
+  const uint32_t* cbm;
+  uint32_t cwords;
 };
 
 // Adjacency list of v: its first element and length.
@@ -111,6 +114,21 @@ __device__ __forceinline__ const uint32_t* HubBitmap(const DGraph& g, uint32_t v
 
 __device__ __forceinline__ bool BitTest(const uint32_t* bm, uint32_t x) {
   return (__ldg(bm + (x >> 5)) >> (x & 31)) & 1u;
+}
+
+// The coarse bitmap of v (null: v is no hub, or none was built).
+__device__ __forceinline__ const uint32_t* HubCoarse(const DGraph& g, uint32_t v) {
+  if (!g.hub || !g.cbm) return nullptr;
+  int32_t s = __ldg(g.hub + v);
+  return s < 0 ? nullptr : g.cbm + (size_t)s * g.cwords;
+}
+
+// Membership in a hub's list: the coarse bit of x's 32-vertex block first
+// (the coarse bitmaps are small enough to stay in L2), the bitmap word only
+// when the block holds a neighbour.
+__device__ __forceinline__ bool BitTest2(const uint32_t* bm, const uint32_t* coarse, uint32_t x) {
+  if (coarse && !((__ldg(coarse + (x >> 10)) >> ((x >> 5) & 31)) & 1u)) return false;
+  return BitTest(bm, x);
 }
 
 __device__ __forceinline__ uint32_t SetIndex(const DFront& F, int u, uint32_t p) {
